@@ -1,0 +1,108 @@
+"""Median-dual geometry on the CPU (oracle; restates ``zvcfd/fv/geometry.py``).
+
+All functions take element node coordinates ``x (E, n, 3)`` of one type.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from zvcfd_b200.topology import tables
+
+
+def element_points(x: np.ndarray, kind: str) -> np.ndarray:
+    """Dual points ``(E, n_pts, 3)`` (``zvcfd/fv/geometry.py:177-179``)."""
+    return np.einsum("pn,enk->epk", tables(kind).weights, x)
+
+
+def ip_areas(P: np.ndarray, kind: str) -> np.ndarray:
+    """Flux-point area vectors ``(E, n_ip, 3)``, edge node a -> b (``geometry.py:182-185``)."""
+    T = P[:, tables(kind).tris]
+    return 0.5 * np.cross(T[:, :, 1] - T[:, :, 0], T[:, :, 2] - T[:, :, 0])
+
+
+def ip_points(P: np.ndarray, kind: str) -> np.ndarray:
+    """Flux-point centroids ``(E, n_ip, 3)`` (``geometry.py:188-190``)."""
+    return P[:, tables(kind).tris].mean(2)
+
+
+def scv_volumes(P: np.ndarray, kind: str) -> np.ndarray:
+    """Sub-control volumes ``(E, n)`` by the divergence theorem (``geometry.py:193-215``)."""
+    t = tables(kind)
+    T = P[:, t.tris]
+    A = 0.5 * np.cross(T[:, :, 1] - T[:, :, 0], T[:, :, 2] - T[:, :, 0])
+    cen = T.mean(2)
+    x = P[:, :t.n]
+    a, b = t.edge[:, 0], t.edge[:, 1]
+    ca = np.einsum("eik,eik->ei", cen - x[:, a], A)
+    cb = -np.einsum("eik,eik->ei", cen - x[:, b], A)
+    Ma = np.zeros((t.n_ip, t.n))
+    Mb = np.zeros((t.n_ip, t.n))
+    Ma[np.arange(t.n_ip), a] = 1.0
+    Mb[np.arange(t.n_ip), b] = 1.0
+    return (ca @ Ma + cb @ Mb) / 3.0
+
+
+def gradients(x: np.ndarray, kind: str) -> np.ndarray:
+    """Shape-function gradients at the flux points ``(E, n_ip, n, 3)`` (``geometry.py:218-223``)."""
+    t = tables(kind)
+    J = np.einsum("enk,ind->eikd", x, t.dN_ip)
+    Jinv = np.linalg.inv(J)
+    return np.einsum("ind,eidk->eink", t.dN_ip, Jinv)
+
+
+def boundary_subfaces(nodes: np.ndarray, faces: np.ndarray) -> np.ndarray:
+    """Each node's share of each boundary face, area vectors ``(F, 4, 3)`` (``geometry.py:226-244``)."""
+    tri = faces[:, 3] < 0
+    out = np.zeros(faces.shape + (3,))
+    for n, sel in ((3, tri), (4, ~tri)):
+        if not sel.any():
+            continue
+        p = nodes[faces[sel, :n]]
+        fc = p.mean(1)
+        rows = np.flatnonzero(sel)
+        for i in range(n):
+            nxt = 0.5 * (p[:, i] + p[:, (i + 1) % n])
+            prv = 0.5 * (p[:, i] + p[:, (i - 1) % n])
+            out[rows, i] = 0.5 * np.cross(fc - p[:, i], prv - nxt)
+    return out
+
+
+def boundary_subface_weights(faces: np.ndarray) -> np.ndarray:
+    """Weights ``(F, 4, 4)`` from face nodes to each sub-face's area centroid (``geometry.py:247-266``)."""
+    tri = faces[:, 3] < 0
+    w = np.zeros(faces.shape + (4,))
+    t = np.full((3, 3), 7.0 / 36.0)
+    np.fill_diagonal(t, 11.0 / 18.0)
+    q = np.array([[9, 3, 1, 3], [3, 9, 3, 1], [1, 3, 9, 3], [3, 1, 3, 9]]) / 16.0
+    w[tri, :3, :3] = t
+    w[~tri] = q
+    return w
+
+
+class ElementGeometry:
+    """Per-type geometry of a mesh (``zvcfd/fv/reference.py:465-474``)."""
+
+    def __init__(self, kind: str, elem: np.ndarray, nodes: np.ndarray):
+        t = tables(kind)
+        self.kind, self.elem, self.t = kind, elem, t
+        x = nodes[elem]
+        P = element_points(x, kind)
+        self.A = ip_areas(P, kind)
+        self.G = gradients(x, kind)
+        self.N = t.N_ip
+        self.xip = ip_points(P, kind)
+        self.scv = scv_volumes(P, kind)
+        self.gbar = self.G.mean(1)
+        self.ea, self.eb = t.edge[:, 0], t.edge[:, 1]
+
+
+def node_volumes(mesh, geoms) -> np.ndarray:
+    V = np.zeros(mesh.n_nodes)
+    for g in geoms:
+        V += np.bincount(g.elem.ravel(), g.scv.ravel(), mesh.n_nodes)
+    return V
+
+
+__all__ = ["ElementGeometry", "boundary_subface_weights", "boundary_subfaces", "element_points",
+           "gradients", "ip_areas", "ip_points", "node_volumes", "scv_volumes"]

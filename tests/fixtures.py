@@ -1,0 +1,105 @@
+"""Loading the golden vectors (``tests/golden/*.npz``) into meshes and solver inputs."""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+from zvcfd_b200.mesh import Mesh, Zone
+from zvcfd_b200.topology import KINDS
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+KERNEL_MESHES = ("tet", "pyramid", "wedge", "hex", "mixed", "delaunay")
+KERNEL_VARIANTS = ("newt_steady", "gn_dt")
+
+
+def load(name: str) -> dict:
+    with np.load(GOLDEN / f"{name}.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def mesh_of(g: dict) -> Mesh:
+    els = {k: g[f"elem_{k}"] for k in KINDS if f"elem_{k}" in g}
+    m = Mesh(g["nodes"], els)
+    for zid, name in zip(g["zone_ids"], g["zone_names"]):
+        m.zones[int(zid)] = Zone(int(zid), "", str(name), g[f"zone_{int(zid)}"])
+    return m
+
+
+def kernel_case(mesh_name: str, variant: str) -> dict:
+    return load(f"kernel_{mesh_name}_{variant}")
+
+
+def mdot_of(g: dict, prefix: str = "mdot") -> dict:
+    return {k: g[f"{prefix}_{k}"] for k in KINDS if f"{prefix}_{k}" in g}
+
+
+def fluid_of(g: dict):
+    from zvcfd_b200.fluid import CarreauYasuda, Fluid
+
+    cy = None
+    if int(g.get("gn", 0)) or "cy" in g and "flow_rate" in g:
+        c = g["cy"]
+        cy = CarreauYasuda(float(c[0]), float(c[1]), float(c[2]), float(c[3]), float(c[4]))
+    return Fluid(float(g["rho"]), float(g["mu"]), viscosity=cy)
+
+
+def oracle_for_kernel_case(g: dict):
+    """The oracle set up as the reference was when the kernel golden case was made."""
+    from oracle.fv import OracleSolver
+
+    m = mesh_of(g)
+    gn = bool(int(g["gn"]))
+    dt = float(g["dt"]) or None
+    s = OracleSolver(m, fluid_of(g), {z: {"kind": "wall"} for z in m.zones},
+                     advection="high-resolution", dt=dt, transpose=gn)
+    s.U, s.P = g["U"].copy(), g["P"].copy()
+    for K in s.kinds:
+        K.mdot = g[f"mdot_{K.kind}"].copy()
+    return s
+
+
+def oracle_kernel_outputs(g: dict) -> dict:
+    """Everything the kernel golden case pins, computed by the oracle."""
+    s = oracle_for_kernel_case(g)
+    rho = float(g["rho"])
+    dt = float(g["dt"]) or None
+    gradU, gradP = s.nodal_gradient(s.U), s.nodal_gradient(s.P)
+    mdot = {K.kind: K.mdot.copy() for K in s.kinds}
+    diag = s.momentum_diagonal()
+    tdiag = rho * s.V / dt if dt else 0.0
+    dnode, snode = s.V / (diag + tdiag), s.V / diag
+    levels = [(1.0, s.U.copy(), mdot)] if dt else []
+    data, b = s.assemble_elements(s.U, mdot, gradU, g["beta_frozen"], gradP, dnode, snode,
+                                  levels)
+    new, imb = s.mass_flows(g["U_new"], g["P_new"], s.nodal_gradient(g["P_new"]), dnode, snode,
+                            [(1.0, g["U"], mdot)] if dt else [])
+    return {"V": s.V, "gradU": gradU, "gradP": gradP, "diag": diag,
+            "beta_limiter": s.limiter(gradU), "indptr": s.indptr, "indices": s.indices,
+            "data_raw": data, "b_raw": b, "imbalance": imb, "mdot_new": new,
+            "dnode": dnode, "snode": snode, "solver": s}
+
+
+def pipe_bcs(name: str, g: dict, m):
+    """The boundary conditions the golden pipe case was solved with."""
+    z = {zz.name: k for k, zz in m.zones.items()}
+    if name == "pipe_reference_tube" or name == "pipe_tet_si":
+        R, umax = float(g["radius"]), float(g["umax"])
+
+        def prof(x):
+            r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+            return np.stack([0 * r2, 0 * r2, umax * np.clip(1 - r2, 0, None)], 1)
+
+        inlet = {"kind": "velocity", "value": prof}
+    else:
+        def shape(x):
+            r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / (2e-3) ** 2
+            return np.clip(1 - r2, 0, None)
+
+        inlet = {"kind": "velocity", "flow_rate": float(g["flow_rate"]), "profile": shape}
+    return {z["inlet"]: inlet, z["outlet"]: {"kind": "pressure", "value": 0.0},
+            z["wall"]: {"kind": "wall"}}
+
+
+PIPES = ("pipe_reference_tube", "pipe_tet_si", "curved_cy")

@@ -1,0 +1,205 @@
+"""Generate the golden vectors of the coupled FV path by running the reference itself.
+
+Run once, in a container where the reference is importable:
+
+    PYTHONPATH=/root/reference:. PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
+
+It writes ``tests/golden/*.npz``: element tables, and for six distorted test
+meshes (every element type) the reference's node volumes, nodal gradients,
+momentum diagonal, limiter, raw assembled block system, pattern and new mass
+flows on a seeded random state (the procedure of the reference's
+``tests/test_fv_fast.py:98-159``), plus converged fields of three small pipes
+solved by the reference's CPU solver with lagged Rhie-Chow. Nothing at test or
+bench time reads the reference: the tests read these files.
+"""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+from zvcfd.fv.geometry import topology  # noqa: E402  (the reference)
+from zvcfd.fv.pattern import node_graph  # noqa: E402
+from zvcfd.fv.reference import Fluid, ReferenceSolver  # noqa: E402
+from zvcfd.mesh.core import BoundaryZone, UnstructuredMesh  # noqa: E402
+from zvcfd.mesh.generate import box, delaunay_box, tube  # noqa: E402
+from zvcfd.rheology import CarreauYasuda  # noqa: E402
+
+from zvcfd_b200 import mesh as zmesh  # noqa: E402
+
+MESHES = {
+    "tet": lambda: box((3, 3, 3), kind="tet", perturb=0.25, seed=1),
+    "pyramid": lambda: box((2, 2, 2), kind="pyramid", perturb=0.15, seed=2),
+    "wedge": lambda: box((3, 3, 3), kind="wedge", perturb=0.25, seed=3),
+    "hex": lambda: box((3, 3, 3), kind="hex", perturb=0.25, seed=4),
+    "mixed": lambda: tube(0.5, 1.0, n_core=2, n_ring=2, n_axial=3, kind="mixed", layers=1,
+                          perturb=0.1),
+    "delaunay": lambda: delaunay_box((3, 3, 3), seed=5),
+}
+VARIANTS = [(False, None), (True, 0.3)]          # (Carreau-Yasuda + transpose, false dt)
+
+
+def mesh_arrays(m) -> dict:
+    out = {"nodes": m.nodes}
+    for k, e in m.elements.items():
+        out[f"elem_{k}"] = e
+    zids = sorted(m.zones)
+    out["zone_ids"] = np.array(zids, np.int64)
+    out["zone_names"] = np.array([m.zones[z].name for z in zids])
+    for z in zids:
+        out[f"zone_{z}"] = m.zones[z].faces
+    return out
+
+
+def to_reference(m: zmesh.Mesh) -> UnstructuredMesh:
+    um = UnstructuredMesh(m.nodes.copy(), {k: v.copy() for k, v in m.elements.items()})
+    um.zones = {zid: BoundaryZone(zid, z.kind, z.name, z.faces.copy(),
+                                  np.zeros(len(z.faces), np.int64))
+                for zid, z in m.zones.items()}
+    return um
+
+
+def blocks_on_pattern(M, indptr, indices) -> np.ndarray:
+    """The 4x4 blocks of a (4N x 4N) sparse matrix at the pattern's positions."""
+    N = len(indptr) - 1
+    rows = np.repeat(np.arange(N), np.diff(indptr))
+    M = M.tocsr()
+    data = np.zeros((len(indices), 4, 4))
+    for r in range(4):
+        for c in range(4):
+            data[:, r, c] = np.asarray(M[4 * rows + r, 4 * indices + c]).reshape(-1)
+    return data
+
+
+def kernel_case(name: str, gn: bool, dt) -> dict:
+    import scipy.sparse as sp
+
+    m = MESHES[name]()
+    rho, mu = 1.3, 0.7
+    cy = CarreauYasuda(mu_0=0.9, mu_inf=0.1, lam=1.5)
+    fl = Fluid(rho, mu, viscosity=cy if gn else None)
+    s = ReferenceSolver(m, fl, {z: {"kind": "wall"} for z in m.zones},
+                        advection="high-resolution", lag_rhie_chow=True, dt=dt, transpose=gn)
+    rng = np.random.default_rng(11)
+    s.U = rng.normal(size=(s.N, 3))
+    s.P = rng.normal(size=s.N)
+    for K in s.kinds:
+        K.mdot = rng.normal(size=K.mdot.shape)
+    s._frozen_beta = rng.uniform(0, 1, (s.N, 3))
+    U0, P0 = s.U.copy(), s.P.copy()
+    mdot0 = {K.kind: K.mdot.copy() for K in s.kinds}
+    beta0 = s._frozen_beta.copy()
+    s._store_old(first=True)
+    s.assemble()
+    M_raw, b_raw = s._raw
+    if dt:
+        t = rho * s.V / dt
+        M_raw = M_raw - sp.diags(np.repeat(t, 4) * np.tile([1, 1, 1, 0], s.N))
+        b_raw = b_raw - np.column_stack([t[:, None] * s.U, np.zeros(s.N)]).reshape(-1)
+    indptr, indices = node_graph(m)
+    gradU, gradP = s.nodal_gradient(U0), s.nodal_gradient(P0)
+    out = mesh_arrays(m)
+    out.update({
+        "rho": rho, "mu": mu, "gn": int(gn), "dt": 0.0 if dt is None else dt,
+        "cy": np.array([cy.mu_0, cy.mu_inf, cy.lam, cy.a, cy.n]),
+        "U": U0, "P": P0, "beta_frozen": beta0,
+        "V": s.V, "gradU": gradU, "gradP": gradP, "diag": s._a_space,
+        "beta_limiter": s._beta(gradU), "indptr": indptr, "indices": indices,
+        "data_raw": blocks_on_pattern(M_raw, indptr, indices), "b_raw": b_raw.reshape(-1, 4),
+    })
+    for k, v in mdot0.items():
+        out[f"mdot_{k}"] = v
+    # mass flows of a new state with the previous one as the old level
+    U_new, P_new = rng.normal(size=(s.N, 3)), rng.normal(size=s.N)
+    s.U, s.P = U_new, P_new
+    s.update_mass_flows()
+    out.update({"U_new": U_new, "P_new": P_new, "imbalance": s._interior_out})
+    for K in s.kinds:
+        out[f"mdot_new_{K.kind}"] = K.mdot
+    return out
+
+
+def pipe_cases() -> dict:
+    """Converged fields of the reference's CPU solver (lagged Rhie-Chow, fixed blend)."""
+    cases = {}
+    # the reference's own pipe test case (tests/test_fv_reference.py:152-162)
+    R = 0.5
+    m = tube(R, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed", layers=1)
+    zid = {z.name: k for k, z in m.zones.items()}
+
+    def prof(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+        return np.stack([0 * r2, 0 * r2, 2 * np.clip(1 - r2, 0, None)], 1)
+
+    bcs = {zid["inlet"]: {"kind": "velocity", "value": prof},
+           zid["outlet"]: {"kind": "pressure", "value": 0.0}, zid["wall"]: {"kind": "wall"}}
+    s = ReferenceSolver(m, Fluid(1.0, 0.2), bcs, advection=1.0, lag_rhie_chow=True)
+    rep = s.solve(max_iterations=400, tol=1e-12)
+    assert rep.converged
+    cases["pipe_reference_tube"] = dict(mesh_arrays(m), U=s.U, P=s.P, rho=1.0, mu=0.2,
+                                        iterations=rep.iterations, radius=R, umax=2.0)
+    # a small jittered tetrahedral pipe in SI units (the plain FP64 Poiseuille pipe, shrunk)
+    R2 = 1e-3
+    pm = zmesh.pipe(R2, 3e-3, n_core=4, n_ring=2, n_axial=6, kind="tet", jitter_amount=0.05,
+                    seed=7)
+    um = to_reference(pm)
+    z = {zz.name: k for k, zz in pm.zones.items()}
+
+    def prof2(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R2 ** 2
+        return np.stack([0 * r2, 0 * r2, 0.2 * np.clip(1 - r2, 0, None)], 1)
+
+    bcs2 = {z["inlet"]: {"kind": "velocity", "value": prof2},
+            z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    s = ReferenceSolver(um, Fluid(1060.0, 3.5e-3), bcs2, advection=1.0, lag_rhie_chow=True)
+    rep = s.solve(max_iterations=400, tol=1e-12)
+    assert rep.converged
+    cases["pipe_tet_si"] = dict(mesh_arrays(pm), U=s.U, P=s.P, rho=1060.0, mu=3.5e-3,
+                                iterations=rep.iterations, radius=R2, umax=0.2)
+    # a small curved tube, hexahedral core and wedge layers, Carreau-Yasuda, flow-rate inlet
+    cm = zmesh.curved_tube(2e-3, 20e-3, np.pi / 2, n_core=4, n_ring=3, n_axial=8, layers=2,
+                           growth=0.8)
+    um = to_reference(cm)
+    z = {zz.name: k for k, zz in cm.zones.items()}
+
+    def shape(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / (2e-3) ** 2
+        return np.clip(1 - r2, 0, None)
+
+    bcs3 = {z["inlet"]: {"kind": "velocity", "flow_rate": 1e-6, "profile": shape},
+            z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    cy = CarreauYasuda()
+    s = ReferenceSolver(um, Fluid(1060.0, 0.0035, viscosity=cy), bcs3, advection=1.0,
+                        lag_rhie_chow=True)
+    rep = s.solve(max_iterations=400, tol=1e-12)
+    assert rep.converged
+    cases["curved_cy"] = dict(mesh_arrays(cm), U=s.U, P=s.P, rho=1060.0, mu=0.0035,
+                              iterations=rep.iterations, flow_rate=1e-6,
+                              cy=np.array([cy.mu_0, cy.mu_inf, cy.lam, cy.a, cy.n]))
+    return cases
+
+
+def main():
+    tabs = {}
+    for k in ("tet", "pyramid", "wedge", "hex"):
+        t = topology(k)
+        tabs.update({f"{k}_edges": t.edges, f"{k}_tris": t.tris, f"{k}_N": t.N_ip,
+                     f"{k}_dN": t.dN_ip, f"{k}_W": t.point_weights, f"{k}_xi": t.xi_ip})
+    np.savez_compressed(HERE / "tables.npz", **tabs)
+    for name in MESHES:
+        for gn, dt in VARIANTS:
+            tag = f"kernel_{name}_{'gn' if gn else 'newt'}_{'dt' if dt else 'steady'}"
+            np.savez_compressed(HERE / f"{tag}.npz", **kernel_case(name, gn, dt))
+            print("wrote", tag)
+    for tag, arrays in pipe_cases().items():
+        np.savez_compressed(HERE / f"{tag}.npz", **arrays)
+        print("wrote", tag, arrays["iterations"])
+
+
+if __name__ == "__main__":
+    main()

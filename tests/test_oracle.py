@@ -1,0 +1,55 @@
+"""The oracle reproduces the reference's own outputs (golden vectors made by the reference)."""
+
+import numpy as np
+import pytest
+
+from fixtures import KERNEL_MESHES, KERNEL_VARIANTS, kernel_case, load, mdot_of, oracle_kernel_outputs
+from zvcfd_b200.topology import KINDS, tables
+
+
+def test_tables_match_reference():
+    g = load("tables")
+    for k in KINDS:
+        t = tables(k)
+        np.testing.assert_array_equal(t.edge, g[f"{k}_edges"])
+        np.testing.assert_array_equal(t.tris, g[f"{k}_tris"])
+        np.testing.assert_array_equal(t.N_ip, g[f"{k}_N"])
+        np.testing.assert_array_equal(t.dN_ip, g[f"{k}_dN"])
+        np.testing.assert_array_equal(t.weights, g[f"{k}_W"])
+
+
+@pytest.mark.parametrize("variant", KERNEL_VARIANTS)
+@pytest.mark.parametrize("name", KERNEL_MESHES)
+def test_oracle_matches_reference_kernels(name, variant):
+    g = kernel_case(name, variant)
+    o = oracle_kernel_outputs(g)
+    np.testing.assert_array_equal(o["indptr"], g["indptr"])
+    np.testing.assert_array_equal(o["indices"], g["indices"])
+    np.testing.assert_allclose(o["V"], g["V"], rtol=1e-12)
+    np.testing.assert_allclose(o["gradU"], g["gradU"], atol=1e-11)
+    np.testing.assert_allclose(o["gradP"], g["gradP"], atol=1e-11)
+    np.testing.assert_allclose(o["diag"], g["diag"], rtol=1e-11, atol=1e-12)
+    np.testing.assert_allclose(o["beta_limiter"], g["beta_limiter"], atol=1e-12)
+    scale = np.abs(g["data_raw"]).max()
+    assert np.abs(o["data_raw"] - g["data_raw"]).max() < 1e-12 * scale
+    np.testing.assert_allclose(o["b_raw"], g["b_raw"], atol=1e-12 * np.abs(g["b_raw"]).max())
+    np.testing.assert_allclose(o["imbalance"], g["imbalance"],
+                               atol=1e-12 * np.abs(g["imbalance"]).max())
+    for k, v in mdot_of(g, "mdot_new").items():
+        np.testing.assert_allclose(o["mdot_new"][k], v, atol=1e-12 * np.abs(v).max())
+
+
+@pytest.mark.parametrize("name", ["pipe_reference_tube", "pipe_tet_si", "curved_cy"])
+def test_oracle_reaches_reference_solution(name):
+    from fixtures import fluid_of, mesh_of, pipe_bcs
+    from oracle.fv import OracleSolver
+
+    g = load(name)
+    m = mesh_of(g)
+    s = OracleSolver(m, fluid_of(g), pipe_bcs(name, g, m), advection=1.0)
+    rep = s.solve(max_iterations=400, tol=1e-12)
+    assert rep["converged"]
+    np.testing.assert_allclose(s.U, g["U"], atol=1e-9 * np.abs(g["U"]).max())
+    np.testing.assert_allclose(s.P, g["P"], atol=1e-9 * np.ptp(g["P"]))
+    flows = s.zone_flows()
+    assert abs(sum(flows.values())) < 1e-11 * sum(abs(v) for v in flows.values())
