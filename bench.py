@@ -1,0 +1,362 @@
+"""Benchmark: FV outer-iteration time and block-SpMV GB/s on one B200, FP64 and mixed precision.
+
+Workload (the plain FP64 steady curved tube): a 90-degree arc tube of radius 2 mm on a bend of
+radius 20 mm, a hexahedral O-grid core with five wedge wall layers graded toward the wall
+(400,686 nodes, 501,600 elements, about 27 blocks per row), Carreau-Yasuda blood
+(rho 1060, mu0 0.056, mu_inf 0.00345, lambda 3.313, a 2, n 0.3568), a parabolic 1 ml/s inlet,
+a zero-pressure outlet, High Resolution advection. Synthetic: the mesh is generated, seeded.
+
+A step is one outer iteration (assembly, boundary pass, AMG-FGMRES to 0.1, update, mass
+flows, one read-back). ``value`` is outer iterations per second over the whole job (N
+independent replicas for N > 1: the path does not shard across GPUs). The matrix (1.4 GB)
+is larger than L2, so no flush is needed between steps.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]``
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "FV outer-iteration time & block-SpMV GB/s, mixed vs FP64 at 1e-8 rel. residual"
+UNIT = "outer-iterations/s"
+WORKLOAD = "curved Carreau-Yasuda tube, 400,686 nodes (hex core + 5 wedge wall layers), steady"
+
+
+def make_case(n_axial=285):
+    from zvcfd_b200.fluid import CarreauYasuda, Fluid
+    from zvcfd_b200.mesh import curved_tube
+
+    R = 2e-3
+    m = curved_tube(R, 20e-3, np.pi / 2, n_core=20, n_ring=12, n_axial=n_axial, layers=5,
+                    growth=0.8)
+    z = {zz.name: k for k, zz in m.zones.items()}
+
+    def shape(x):
+        return np.clip(1.0 - (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2, 0.0, None)
+
+    bcs = {z["inlet"]: {"kind": "velocity", "flow_rate": 1e-6, "profile": shape},
+           z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    return m, Fluid(1060.0, 0.00345, viscosity=CarreauYasuda()), bcs
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            f = [v.strip() for v in ln.split(",")]
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def spmv_roofline(solver, reps=20):
+    """Time the FP64 and FP32 block-CSR SpMV on the assembled matrix with CUDA events."""
+    import torch
+
+    from zvcfd_b200._lib import call, ptr, stream_ptr
+
+    A, _, _, _ = solver._assemble_fused()
+    n, nnzb = A.n, A.nnzb
+    lanes = 16
+    x = torch.randn(n * 4, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    d32 = A.data.reshape(-1).float()
+    x32, y32 = x.float(), torch.empty(n * 4, dtype=torch.float32, device="cuda")
+    out = {}
+    for name, fn, nbytes in (
+            ("fp64", lambda: call("zvfv_bsr_spmv", n, ptr(A.indptr), ptr(A.indices), ptr(A.data),
+                                  ptr(x), ptr(y), lanes, stream_ptr()),
+             132 * nnzb + 72 * n + 8),
+            ("fp32", lambda: call("zvfv_bsr_spmv_f32", n, ptr(A.indptr), ptr(A.indices),
+                                  ptr(d32), ptr(x32), ptr(y32), lanes, stream_ptr()),
+             68 * nnzb + 8 * (n + 1) + 32 * n)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        out[name] = {"seconds": t, "bytes": nbytes, "gbs": nbytes / t / 1e9}
+    return out, n, nnzb
+
+
+def cpu_sample(n_axial=8, steps=1, warmup=1):
+    """The oracle's outer iteration (assembly + ACM-FGMRES to 0.1 + mass flows) on a shorter
+    tube of the same cross-section; returns seconds per outer iteration and the node count."""
+    from oracle.fv import OracleSolver
+    from oracle.linear import ACM, fgmres
+
+    m, fl, bcs = make_case(n_axial)
+    s = OracleSolver(m, fl, bcs)
+
+    def lin(data, b, x0):
+        acm = ACM().setup(s.indptr, s.indices, data)
+        A = s.to_csr(data)
+        x, *_ = fgmres(lambda v: A @ v, b, x0, acm.vcycle, rtol=0.1, maxiter=200)
+        return x
+
+    s.solve(max_iterations=warmup, tol=0.0, linear=lin)
+    t = time.perf_counter()
+    s.solve(max_iterations=steps, tol=0.0, linear=lin)
+    return (time.perf_counter() - t) / steps, m.n_nodes
+
+
+def cpu_spmv_gbs(indptr, indices, data, reps=3):
+    import scipy.sparse as sp
+
+    n = len(indptr) - 1
+    M = sp.bsr_matrix((data.reshape(-1, 4, 4), indices, indptr), shape=(4 * n, 4 * n))
+    x = np.random.default_rng(0).normal(size=4 * n)
+    M @ x
+    t = time.perf_counter()
+    for _ in range(reps):
+        M @ x
+    t = (time.perf_counter() - t) / reps
+    return (132 * len(indices) + 72 * n + 8) / t / 1e9
+
+
+def reference_arm(args, rank, world):
+    """The reference's CPU algorithm (the oracle port) on the host cores, rank 0 only."""
+    if rank != 0:
+        return
+    full_nodes = 400686
+    times = []
+    n_nodes = None
+    for i in range(args.warmup + args.steps):
+        t, n_nodes = cpu_sample(n_axial=args.cpu_axial, steps=1, warmup=1 if i == 0 else 0)
+        if i >= args.warmup:
+            times.append(t)
+    per = float(np.mean(times)) * full_nodes / n_nodes
+    value = 1.0 / per
+    sample = (f"oracle outer iteration (NumPy assembly + ACM-FGMRES to 0.1) on the same tube "
+              f"with {args.cpu_axial} axial cells ({n_nodes} nodes), time scaled by node count "
+              f"to {full_nodes} nodes")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "precision": "fp64", "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_steps(solver, steps):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    recs = [solver.iterate() for _ in range(steps)]
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, recs
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--axial", type=int, default=285, help="axial cells (285: the full tube)")
+    ap.add_argument("--cpu-axial", type=int, default=8, help="axial cells of the CPU sample")
+    ap.add_argument("--no-converge", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from zvcfd_b200._lib import lib
+    from zvcfd_b200.solver import B200Solver
+
+    m, fl, bcs = make_case(args.axial)
+    solver = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1)
+    for _ in range(args.warmup):
+        solver.iterate()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.zvfv_launch_count()
+    with Clocks(local) as clk:
+        elapsed, recs = run_steps(solver, args.steps)
+    launches = lib.zvfv_launch_count() - l0
+    if dist:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        dist.barrier()
+    per = elapsed / args.steps
+    value = world * args.steps / elapsed
+    # end to end through the public API: host state in, one outer iteration, host state out
+    N = m.n_nodes
+    Uh = torch.empty((N, 3), dtype=torch.float64, pin_memory=True)
+    Ph = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    Uh.copy_(solver.U)
+    Ph.copy_(solver.P)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solver.U.copy_(Uh, non_blocking=True)
+        solver.P.copy_(Ph, non_blocking=True)
+        solver.iterate()
+        Uh.copy_(solver.U, non_blocking=True)
+        Ph.copy_(solver.P, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e = args.steps / (time.perf_counter() - t0) * world
+    # mixed precision on the same case
+    mixed = B200Solver(m, fl, bcs, linear="b200-mixed", linear_rtol=0.1)
+    for _ in range(args.warmup):
+        mixed.iterate()
+    melapsed, mrecs = run_steps(mixed, args.steps)
+    extra = {"fp64_linear_iterations": [r["linear_iterations"] for r in recs],
+             "mixed": {"ms_per_step": melapsed / args.steps * 1e3,
+                       "outer_iterations_per_s": args.steps / melapsed,
+                       "speedup_vs_fp64": elapsed / melapsed,
+                       "linear_iterations": [r["linear_iterations"] for r in mrecs]}}
+    # SpMV roofline on the assembled matrix
+    sp, n, nnzb = spmv_roofline(solver)
+    peak, peak_kind = peaks()
+    roof = {"kernel": "k_bsr_spmv<16> fp64", "bound": "hbm", "achieved": sp["fp64"]["gbs"],
+            "peak": peak, "unit": "GB/s", "frac": sp["fp64"]["gbs"] / peak,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6.65 TB/s",
+            "algorithmic_bytes": sp["fp64"]["bytes"], "traffic": None}
+    extra["spmv"] = {"fp64_gbs": sp["fp64"]["gbs"], "fp32_gbs": sp["fp32"]["gbs"],
+                     "fp64_us": sp["fp64"]["seconds"] * 1e6, "fp32_us": sp["fp32"]["seconds"] * 1e6,
+                     "nnzb": nnzb, "rows": n}
+    if not args.no_converge and rank == 0:
+        conv = {}
+        for tag, lin in (("fp64", "b200"), ("mixed", "b200-mixed")):
+            s = B200Solver(m, fl, bcs, linear=lin, linear_rtol=0.1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rep = s.solve(max_iterations=400, tol=1e-8)
+            torch.cuda.synchronize()
+            conv[tag] = {"outer_iterations": rep["iterations"], "converged": rep["converged"],
+                         "seconds": time.perf_counter() - t0,
+                         "final_rms": max(rep["history"][-1][f"rms_{c}"] for c in "uvwp"),
+                         "fields": s.fields()}
+            s.close()
+        f64, fmx = conv["fp64"].pop("fields"), conv["mixed"].pop("fields")
+        conv["mixed"]["field_error_vs_fp64"] = {
+            "U": float(np.linalg.norm(fmx["U"] - f64["U"]) / np.linalg.norm(f64["U"])),
+            "P": float(np.linalg.norm(fmx["P"] - f64["P"]) / np.linalg.norm(f64["P"]))}
+        extra["to_1e-8"] = conv
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        t_cpu, n_cpu = cpu_sample(args.cpu_axial)
+        per_cpu = t_cpu * N / n_cpu
+        A, _, _, _ = solver._assemble_fused()
+        gbs = cpu_spmv_gbs(A.indptr.cpu().numpy(), A.indices.cpu().numpy(),
+                           A.data.cpu().numpy())
+        cpu = {"value": 1.0 / per_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"oracle outer iteration on the same tube with {args.cpu_axial} axial "
+                         f"cells ({n_cpu} nodes), scaled by node count; SciPy BSR SpMV on the "
+                         f"full matrix: {gbs:.2f} GB/s",
+               "spmv_gbs": gbs}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "nodes": N, "blocks": nnzb,
+                           "precision": "fp64 (mixed below)", "linear_rtol": 0.1,
+                           "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32 * N,
+                        "d2h_bytes_per_step": 32 * N + 8 * 29},
+                "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clk.summary(), **extra}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    mixed.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

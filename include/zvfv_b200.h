@@ -1,0 +1,211 @@
+/*
+ * zvfv_b200.h — C ABI of libzvfv_b200.so, the B200 (sm_100a) coupled finite-volume solve path.
+ *
+ * Conventions (those of the reference's AmgX binding, zvcfd/fv/linear.py:681-955, and of its
+ * CuPy kernel launches): every array is a raw device pointer; sizes are int64_t; every entry
+ * point returns an int status (0 = success, see ZVFV_* below) and zvfv_last_error() gives the
+ * message of the last failure on the calling thread; `stream` is a cudaStream_t (NULL = the
+ * legacy default stream). Nothing synchronises the stream unless its comment says so.
+ * Element types: 0 tet, 1 pyramid, 2 wedge, 3 hex (VTK local node order). Per-type element
+ * arrays are in "slot" order (elements sorted by colour) and the per-colour launches take
+ * the host array colour_offsets[n_colours + 1] of first slots.
+ */
+#ifndef ZVFV_B200_H
+#define ZVFV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ZVFV_OK = 0,
+    ZVFV_BAD_ARGUMENT = 1,
+    ZVFV_CUDA_FAILURE = 2,
+    ZVFV_OUT_OF_MEMORY = 3,
+    ZVFV_NOT_CONVERGED = 4,
+    ZVFV_TIMED_OUT = 5,
+    ZVFV_NON_FINITE = 6,
+    ZVFV_UNSUPPORTED = 7
+};
+
+/* ---------------------------------------------------------------- library */
+
+const char *zvfv_last_error(void);
+int zvfv_version(void);
+/* kernels this library has launched since the process started */
+int64_t zvfv_launch_count(void);
+/* doubles per stored geometry record of an element type (zvcfd/fv/fast.py:150-152) */
+int zvfv_record_doubles(int kind);
+
+/* ---------------------------------------------------------------- once-per-mesh setup */
+
+/* The block pattern: sorted unique (row, col) node pairs of all elements, self included.
+ * Replaces zvcfd/fv/fast.py:133-147 gpu_node_graph (host form zvcfd/fv/pattern.py:18-33).
+ * create builds it in a handle and reports nnzb (synchronises the stream); fill writes
+ * indptr int64 (N+1) and indices int32 (nnzb) into caller memory; destroy frees the handle. */
+int zvfv_pattern_create(void **handle, int64_t n_nodes, int n_kinds, const int32_t *const *conn,
+                        const int64_t *n_elems, const int32_t *nodes_per, int64_t *nnzb,
+                        void *stream);
+int zvfv_pattern_fill(void *handle, int64_t *indptr, int32_t *indices, void *stream);
+int zvfv_pattern_destroy(void *handle);
+
+/* Element colouring, bit-exact with zvcfd/fv/fast.py:84-130 gpu_colour (kernels
+ * colour_claim/colour_pick, zvcfd/fv/fast.py:35-70): colour int32 (E), *n_colours on the host.
+ * Synchronises the stream once per round. */
+int zvfv_colour(const int32_t *conn, int n, int64_t E, int64_t n_nodes, int words,
+                int32_t *colour, int32_t *n_colours, int64_t max_rounds, void *stream);
+
+/* Slot order argsort(colour * E + e) and colour offsets (zvcfd/fv/fast.py:199-203):
+ * order int64 (E, slot -> element), offsets int64 (n_colours + 1) on the device. */
+int zvfv_slot_order(const int32_t *colour, int64_t E, int32_t n_colours, int64_t *order,
+                    int64_t *offsets, void *stream);
+
+/* dst[r] = src[idx[r]] (scatter = 0) or dst[idx[r]] = src[r] (scatter = 1), rows of `width`
+ * bytes: FastAssembler.to_slots / from_slots (zvcfd/fv/fast.py:276-290). */
+int zvfv_permute_rows(const void *src, const int64_t *idx, int64_t rows, int64_t width, void *dst,
+                      int scatter, void *stream);
+
+/* Geometry records of every slot (kernel geobuild, zvcfd/fv/_cuda_fast.py:169-188). */
+int zvfv_geobuild(int kind, const int32_t *conn, int64_t n_slots, const double *X, double *geo,
+                  void *stream);
+
+/* Pattern position of every (row, col) pair of every slot (kernel blockpos,
+ * zvcfd/fv/_cuda_fast.py:605-623); pos int32 (E * n * n). */
+int zvfv_blockpos(int kind, const int32_t *conn, int64_t n_slots, const int64_t *indptr,
+                  const int32_t *indices, int32_t *pos, void *stream);
+
+/* Node volumes, Newtonian viscous diagonal, nodal-gradient operator (kernel statics,
+ * zvcfd/fv/_cuda_fast.py:191-236); accumulates into vol (N), dvisc (N), gop (nnzb * 3). */
+int zvfv_statics(int kind, int stored, const int32_t *conn, int n_colours,
+                 const int64_t *colour_offsets, const double *X, const double *geo,
+                 const int32_t *pos, double mu, int transpose, double *vol, double *dvisc,
+                 double *gop, void *stream);
+
+/* ---------------------------------------------------------------- per outer iteration */
+
+/* Nodal gradients of nc <= 4 fields through the gradient operator (kernel csr_gradient,
+ * zvcfd/fv/_cuda_fast.py:627-651, FastAssembler.gradient zvcfd/fv/fast.py:310-325), with the
+ * symmetry-plane mirror of zvcfd/fv/solver.py:441-457 applied when sym (N*3 uint8) is given;
+ * the first nvec fields form a vector. out (N, nc, 3). */
+int zvfv_gradient(int64_t n, int nc, int nvec, const int64_t *indptr, const int32_t *indices,
+                  const double *gop, const double *phi, const uint8_t *sym, double *out,
+                  void *stream);
+
+/* Neighbour extremes of U over the pattern (kernel csr_minmax, zvcfd/fv/_cuda_fast.py:653-667). */
+int zvfv_minmax(int64_t n, const int64_t *indptr, const int32_t *indices, const double *U,
+                double *lo, double *hi, void *stream);
+
+/* Barth-Jespersen blend (kernel limiter, zvcfd/fv/_cuda_fast.py:555-603; FastAssembler.limiter
+ * zvcfd/fv/fast.py:394-406); beta (N*3) initialised to 1 by the caller, min-accumulated. */
+int zvfv_limiter(int kind, int stored, const int32_t *conn, int n_colours,
+                 const int64_t *colour_offsets, const double *X, const double *geo,
+                 const double *U, const double *gradU, const double *lo, const double *hi,
+                 double *beta, void *stream);
+
+/* Momentum diagonal a_P (kernel diag, zvcfd/fv/_cuda_fast.py:239-299; FastAssembler.diagonal
+ * zvcfd/fv/fast.py:327-337); accumulates into out (N). rheo 0 Newtonian, 1 Carreau-Yasuda. */
+int zvfv_diagonal(int kind, int stored, const int32_t *conn, int n_colours,
+                  const int64_t *colour_offsets, const double *X, const double *geo,
+                  const double *mdot, const double *U, int rheo, double mu0, double muinf,
+                  double lam, double ca, double cn, int transpose, int stokes, int has_mut,
+                  const double *mut, double *out, void *stream);
+
+/* Blocks and right-hand side of the flux points, lagged Rhie-Chow (kernel assemble,
+ * zvcfd/fv/_cuda_fast.py:301-467; FastAssembler.assemble zvcfd/fv/fast.py:339-360);
+ * accumulates into data (nnzb * 16) and b (N * 4). */
+int zvfv_assemble(int kind, int stored, const int32_t *conn, int n_colours,
+                  const int64_t *colour_offsets, const double *X, const double *geo,
+                  const double *U, const double *mdot, const double *gradU, const double *beta,
+                  const double *gradP, const double *dnode, const double *snode, int nlev,
+                  double c1, const double *Uo1, const double *mo1, double c2, const double *Uo2,
+                  const double *mo2, double rho, int rheo, double mu0, double muinf, double lam,
+                  double ca, double cn, int transpose, int stokes, int has_mut, const double *mut,
+                  const int32_t *own, const int32_t *pos, double *data, double *b, void *stream);
+
+/* Rhie-Chow mass flows (slot order), net interior outflow and advective diagonal (kernel
+ * massflow, zvcfd/fv/_cuda_fast.py:469-553; FastAssembler.massflow zvcfd/fv/fast.py:380-392);
+ * writes mdot (E * nip), accumulates imbalance and adv (N). */
+int zvfv_massflow(int kind, int stored, const int32_t *conn, int n_colours,
+                  const int64_t *colour_offsets, const double *X, const double *geo,
+                  const double *U, const double *P, const double *gradP, const double *dnode,
+                  const double *snode, int nlev, double c1, const double *Uo1, const double *mo1,
+                  double c2, const double *Uo2, const double *mo2, double rho, double *mdot,
+                  double *imbalance, double *adv, void *stream);
+
+/* Boundary rows, raw-row copy, Dirichlet with symmetric elimination, residual partials and
+ * dimensionless row scaling (kernel finalise, zvcfd/fv/_cuda_bc.py:32-138, launched at
+ * zvcfd/fv/solver.py:669-677). partial: zvfv_finalise_partials(n) rows of 8 doubles. */
+int64_t zvfv_finalise_partials(int64_t n);
+int zvfv_finalise(int64_t n, const int64_t *indptr, const int32_t *indices, const int64_t *dpos,
+                  double *data, double *b, int has_time, const double *tdiag, const double *trhs,
+                  const double *fV, const double *force, const double *inflow, const double *mb,
+                  const double *wcons, const double *wonly, const double *wstab, int stokes,
+                  const double *snl, const uint8_t *fixed, const uint8_t *known,
+                  const double *vel, const double *pval, int eliminate, const int64_t *rawoff,
+                  double *rawdata, double *rawb, const double *x, const double *aP,
+                  const double *V, double rho, const double *scal, const double *lscale,
+                  double *rs_out, double *partial, void *stream);
+
+/* U, P <- x with change partials (kernel update, zvcfd/fv/_cuda_bc.py:140-175, launched at
+ * zvcfd/fv/solver.py:900-902). partial: zvfv_update_partials(n) rows of 5 doubles. */
+int64_t zvfv_update_partials(int64_t n);
+int zvfv_update(int64_t n, const double *x, double *U, double *P, double *partial, void *stream);
+
+/* Deterministic column folds of partial rows: ops[c] 0 sum, 1 max, 2 min (the host reductions
+ * of zvcfd/fv/solver.py:903-908, on the device). */
+int zvfv_fold(int64_t nrows, int width, const double *partial, const int32_t *ops, double *out,
+              void *stream);
+
+/* ---------------------------------------------------------------- block-CSR products */
+
+/* y = A x for 4x4 block CSR (kernel bsr_mv, zvcfd/fv/linear.py:47-61; BlockMatrix.matvec
+ * :93-103 without the rank-one terms); lanes per block row: 4, 8, 16 or 32. */
+int zvfv_bsr_spmv(int64_t n, const int64_t *indptr, const int32_t *indices, const double *data,
+                  const double *x, double *y, int lanes, void *stream);
+/* r = b - A x (the residual form of the same product) */
+int zvfv_bsr_residual(int64_t n, const int64_t *indptr, const int32_t *indices,
+                      const double *data, const double *x, const double *b, double *r, int lanes,
+                      void *stream);
+/* y = A x with FP32 blocks and vectors (the mixed-precision hierarchy's product; AmgX mode
+ * dDFI's matrix precision, zvcfd/fv/linear.py:525, :854-855) */
+int zvfv_bsr_spmv_f32(int64_t n, const int64_t *indptr, const int32_t *indices,
+                      const float *data, const float *x, float *y, int lanes, void *stream);
+
+/* ---------------------------------------------------------------- linear back end */
+
+/* FGMRES preconditioned by one V-cycle of a device-built aggregation AMG: replaces the AmgX C
+ * API the reference binds (AMGX_config_create / resources / matrix / solver handles,
+ * zvcfd/fv/linear.py:728-739, :846-868, :905-955) and its own ACM (linear.py:328-518).
+ * create: precision 0 FP64, 1 FP32 hierarchy; strength 0 block norm, 1 pressure entry. */
+int zvfv_solver_create(void **handle, int precision, int strength, int passes, int presweeps,
+                       int postsweeps, double omega, int coarse_sweeps, int max_levels,
+                       int rebuild_every, int restart);
+/* structure on the first call (or when it changes), coefficients after: AMGX_matrix_upload_all
+ * / AMGX_matrix_replace_coefficients + AMGX_solver_setup (zvcfd/fv/linear.py:327-349, :310) */
+int zvfv_solver_setup(void *handle, int64_t n, int64_t nnzb, const int64_t *indptr,
+                      const int32_t *indices, const double *data, void *stream);
+/* x (in: x0, out: solution) to a reduction rtol of the initial residual, with n_lowrank
+ * rank-one terms u w^T (BlockMatrix.lowrank, zvcfd/fv/linear.py:81-103): AMGX_solver_solve
+ * (linear.py:401-436) / fgmres (linear.py:172-320). Synchronises once per Krylov step. */
+int zvfv_solver_solve(void *handle, const double *b, double *x, double rtol, int maxiter,
+                      int n_lowrank, const int64_t *const *u_idx, const double *const *u_val,
+                      const int64_t *u_len, const int64_t *const *w_idx, const double *const *w_val,
+                      const int64_t *w_len, int *iterations, double *residual, int *converged,
+                      void *stream);
+/* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:386-399) */
+int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
+/* hierarchy sizes (ACM.stats, zvcfd/fv/linear.py:513-518) */
+int zvfv_solver_stats(void *handle, int max_levels, int *levels, int64_t *rows, int64_t *blocks);
+/* one level's size and aggregates (agg: n int32 entries, or NULL) */
+int zvfv_solver_level(void *handle, int level, int64_t *n, int64_t *nnzb, int64_t *n_coarse,
+                      int32_t *agg, void *stream);
+/* AMGX_solver_destroy / matrix / vector / resources (zvcfd/fv/linear.py:351-384) */
+int zvfv_solver_destroy(void *handle);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZVFV_B200_H */

@@ -1,0 +1,44 @@
+"""The C-ABI library loads without a GPU and exports every entry point include/*.h declares."""
+
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(zvfv_\w+)\s*\(", text))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    from zvcfd_b200 import _lib
+
+    names = declared_symbols()
+    assert len(names) > 25
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    for n in sorted(names):
+        assert hasattr(lib, n), n
+    # the ctypes binding declares exactly the header's entry points
+    assert set(_lib.declared()) == names
+
+
+def test_library_reports_errors_without_a_gpu():
+    from zvcfd_b200 import _lib
+
+    assert _lib.lib.zvfv_version() >= 1
+    assert _lib.lib.zvfv_record_doubles(3) == 728          # hex: 2*24*3 + 24*8*3 + 8
+    assert _lib.lib.zvfv_record_doubles(0) == 88            # tet (one gradient set)
+    # argument checks run before any CUDA call
+    rc = _lib.lib.zvfv_gradient(10, 5, 0, None, None, None, None, None, None, None)
+    assert rc == 1 and b"nc" in _lib.lib.zvfv_last_error()
+
+
+def test_tables_header_is_current():
+    from zvcfd_b200.topology import HEADER_PATH, header_source
+
+    assert HEADER_PATH.read_text() == header_source()

@@ -1,0 +1,477 @@
+// Aggregation multigrid for the coupled 4x4 block system, set up and applied on the device.
+//
+// The method is the reference's own additive-correction multigrid (ACM,
+// zvcfd/fv/linear.py:328-518; Hutchinson & Raithby 1986, Notay 2010 pairwise aggregation):
+//
+//  * aggregation: pairwise matching on coupling strength, `passes` times per level (about
+//    4:1), each pass: up to four rounds in which every free node picks its strongest free
+//    neighbour (ties: the smallest column) and mutual picks (i < j) become pairs numbered in
+//    order of i; then unmatched nodes join their strongest aggregated neighbour, and the
+//    rest stay single (linear.py:373-413). Between passes the graph is coarsened by summing
+//    strengths per aggregate pair (linear.py:415-433). Strength is the block's Frobenius norm
+//    over the geometric mean of the two diagonal blocks' (ACM), or the pressure-pressure
+//    entry in the same form (AmgX's `aggregation_edge_weight_component: 3`, linear.py:95-102);
+//  * coarse operators: Galerkin with piecewise-constant transfer, the sum of the blocks of
+//    each aggregate pair (linear.py:437-454), in a fixed order (deterministic);
+//  * smoothing: damped block Jacobi with the inverse of each 4x4 diagonal block;
+//  * coarsest level: the explicit inverse of the dense matrix (Gauss-Jordan with partial
+//    pivoting in one CTA), or smoothing sweeps when coarsening stalls above that size.
+//
+// The hierarchy is always built in FP64; the V-cycle runs in FP64, or in FP32 with FP32
+// copies of every level's blocks and diagonal inverses (the mixed-precision form: half the
+// bytes per cycle, with FP64 kept in the outer FGMRES).
+#pragma once
+
+#include <cub/cub.cuh>
+
+#include <vector>
+
+#include "devmem.cuh"
+#include "spmv.cuh"
+
+namespace zvfv {
+namespace amg {
+
+constexpr int DENSE_MAX = 32;            // block rows of a dense coarsest level (128 x 128)
+
+// ------------------------------------------------------------------ small kernels
+
+__global__ void k_iota64(long long *p, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = i;
+}
+
+__global__ void k_fill_int(int *p, long long n, int v) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// strength measure of every block: Frobenius norm (mode 0) or |pressure-pressure| (mode 1)
+__global__ void k_block_weight(long long nnz, const double *__restrict__ data, int mode,
+                               double *__restrict__ w) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nnz) return;
+    const double *b = data + p * 16;
+    if (mode == 1) {
+        w[p] = fabs(b[15]);
+        return;
+    }
+    double s = 0.0;        // products rounded separately (no contraction): reproducible on the CPU
+#pragma unroll
+    for (int e = 0; e < 16; ++e) s = __dadd_rn(s, __dmul_rn(b[e], b[e]));
+    w[p] = sqrt(s);
+}
+
+// row of every entry (CSR)
+__global__ void k_rows_of(long long n, const long long *__restrict__ indptr, long long *__restrict__ row) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (long long p = indptr[i]; p < indptr[i + 1]; ++p) row[p] = i;
+}
+
+// diagonal weight per row (0 if the row has no diagonal entry) and diagonal position
+__global__ void k_diag_of(long long n, const long long *__restrict__ indptr, const int *__restrict__ idx,
+                          const double *__restrict__ w, double *__restrict__ dw,
+                          long long *__restrict__ dpos) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    long long pd = -1;
+    for (long long p = indptr[i]; p < indptr[i + 1]; ++p)
+        if (idx[p] == i) {
+            pd = p;
+            if (w) d = w[p];
+        }
+    if (dw) dw[i] = d;
+    if (dpos) dpos[i] = pd;
+}
+
+__global__ void k_strength(long long nnz, const long long *__restrict__ row, const int *__restrict__ col,
+                           const double *__restrict__ w, const double *__restrict__ dw,
+                           double *__restrict__ s) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nnz) return;
+    s[p] = w[p] / sqrt(fmax(dw[row[p]] * dw[col[p]], 1e-300));
+}
+
+// every free node's strongest free off-diagonal neighbour (first maximum in column order)
+__global__ void k_best_free(long long n, const long long *__restrict__ indptr, const int *__restrict__ idx,
+                            const double *__restrict__ s, const int *__restrict__ agg,
+                            int *__restrict__ best, int *__restrict__ any) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int b = -1;
+    if (agg[i] < 0) {
+        double bs = 0.0;
+        for (long long p = indptr[i]; p < indptr[i + 1]; ++p) {
+            const int j = idx[p];
+            if (j == i || agg[j] >= 0) continue;
+            if (b < 0 || s[p] > bs) { b = j; bs = s[p]; }
+        }
+    }
+    best[i] = b;
+    if (b >= 0) *any = 1;
+}
+
+__global__ void k_leaders(long long n, const int *__restrict__ best, int *__restrict__ flag) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = best[i];
+    flag[i] = (j >= 0 && j > i && best[j] == i) ? 1 : 0;
+}
+
+// pairs (i, best[i]) with leader flags take ids nxt + rank (exclusive scan of flags)
+__global__ void k_assign_pairs(long long n, const int *__restrict__ best, const int *__restrict__ flag,
+                               const int *__restrict__ rank, const int *__restrict__ nxt,
+                               int *__restrict__ agg) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !flag[i]) return;
+    const int id = *nxt + rank[i];
+    agg[i] = id;
+    agg[best[i]] = id;
+}
+
+__global__ void k_advance(const int *__restrict__ flag, const int *__restrict__ rank, long long n,
+                          int *__restrict__ nxt) {
+    if (n > 0) *nxt += rank[n - 1] + flag[n - 1];
+}
+
+// unmatched nodes: the aggregate of their strongest aggregated neighbour, or -1
+__global__ void k_join(long long n, const long long *__restrict__ indptr, const int *__restrict__ idx,
+                       const double *__restrict__ s, const int *__restrict__ agg,
+                       int *__restrict__ join) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int to = -1;
+    if (agg[i] < 0) {
+        double bs = 0.0;
+        int bj = -1;
+        for (long long p = indptr[i]; p < indptr[i + 1]; ++p) {
+            const int j = idx[p];
+            if (agg[j] < 0) continue;             // also skips i itself
+            if (bj < 0 || s[p] > bs) { bj = j; bs = s[p]; }
+        }
+        if (bj >= 0) to = agg[bj];
+    }
+    join[i] = to;
+}
+
+__global__ void k_apply_join(long long n, const int *__restrict__ join, int *__restrict__ agg,
+                             int *__restrict__ single) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool free_ = agg[i] < 0;
+    single[i] = (free_ && join[i] < 0) ? 1 : 0;
+    if (free_ && join[i] >= 0) agg[i] = join[i];
+}
+
+__global__ void k_assign_singles(long long n, const int *__restrict__ single, const int *__restrict__ rank,
+                                 const int *__restrict__ nxt, int *__restrict__ agg) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && single[i]) agg[i] = *nxt + rank[i];
+}
+
+__global__ void k_compose(long long n, const int *__restrict__ a, int *__restrict__ total) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) total[i] = a[total[i]];
+}
+
+__global__ void k_pair_key(long long m, const long long *__restrict__ row, const int *__restrict__ col,
+                           const int *__restrict__ agg, unsigned long long nc,
+                           unsigned long long *__restrict__ key) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < m) key[p] = (unsigned long long)agg[row[p]] * nc + (unsigned long long)agg[col[p]];
+}
+
+__global__ void k_int_key(long long m, const int *__restrict__ a, unsigned long long *__restrict__ key) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < m) key[p] = (unsigned long long)a[p];
+}
+
+__global__ void k_seg_flags(long long m, const unsigned long long *__restrict__ k, int *__restrict__ f) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < m) f[p] = (p == 0 || k[p] != k[p - 1]) ? 1 : 0;
+}
+
+__global__ void k_seg_starts(long long m, const int *__restrict__ f, const int *__restrict__ rank,
+                             const unsigned long long *__restrict__ k, long long *__restrict__ seg,
+                             unsigned long long *__restrict__ ukey) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < m && f[p]) {
+        seg[rank[p]] = p;
+        ukey[rank[p]] = k[p];
+    }
+}
+
+__global__ void k_seg_end(long long m, long long nseg, long long *__restrict__ seg) {
+    seg[nseg] = m;
+}
+
+// CSR of unique sorted keys key = row * nc + col
+__global__ void k_keys_to_csr(long long nseg, long long nrows, unsigned long long nc,
+                              const unsigned long long *__restrict__ ukey, long long *__restrict__ indptr,
+                              int *__restrict__ idx) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nseg) idx[i] = (int)(ukey[i] % nc);
+    if (i <= nrows) {
+        if (i == nrows) { indptr[nrows] = nseg; return; }
+        const unsigned long long target = (unsigned long long)i * nc;
+        long long lo = 0, hi = nseg;
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            if (ukey[mid] < target) lo = mid + 1; else hi = mid;
+        }
+        indptr[i] = lo;
+    }
+}
+
+// segmented sums of width-W rows in segment order (the original order inside a segment)
+__global__ void k_seg_sum(long long nseg, int W, const long long *__restrict__ seg,
+                          const long long *__restrict__ perm, const double *__restrict__ src,
+                          double *__restrict__ dst) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nseg * W) return;
+    const long long s = t / W;
+    const int c = (int)(t % W);
+    double acc = 0.0;
+    for (long long q = seg[s]; q < seg[s + 1]; ++q) acc += src[perm[q] * W + c];
+    dst[t] = acc;
+}
+
+// inverse of every row's 4x4 diagonal block (Gauss-Jordan, partial pivoting); a singular
+// block leaves a zero inverse (the row is then not smoothed)
+template <typename V>
+__global__ void k_dinv(long long n, const double *__restrict__ data, const long long *__restrict__ dpos,
+                       V *__restrict__ dinv) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a[4][8];
+    const long long pd = dpos[i];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            a[r][c] = pd >= 0 ? data[pd * 16 + r * 4 + c] : 0.0;
+            a[r][4 + c] = r == c ? 1.0 : 0.0;
+        }
+    bool ok = pd >= 0;
+    for (int k = 0; k < 4 && ok; ++k) {
+        int piv = k;
+        for (int r = k + 1; r < 4; ++r)
+            if (fabs(a[r][k]) > fabs(a[piv][k])) piv = r;
+        if (!(fabs(a[piv][k]) > 0.0)) { ok = false; break; }
+        if (piv != k)
+            for (int c = 0; c < 8; ++c) { const double t = a[k][c]; a[k][c] = a[piv][c]; a[piv][c] = t; }
+        const double inv = 1.0 / a[k][k];
+        for (int c = 0; c < 8; ++c) a[k][c] *= inv;
+        for (int r = 0; r < 4; ++r) {
+            if (r == k) continue;
+            const double f = a[r][k];
+            if (f != 0.0)
+                for (int c = 0; c < 8; ++c) a[r][c] -= f * a[k][c];
+        }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) dinv[i * 16 + r * 4 + c] = (V)(ok ? a[r][4 + c] : 0.0);
+}
+
+template <typename A, typename B>
+__global__ void k_convert(long long n, const A *__restrict__ src, B *__restrict__ dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (B)src[i];
+}
+
+// dense (4n x 4n) copy of a small block-CSR matrix, column-major free: row-major
+__global__ void k_densify(long long n, const long long *__restrict__ indptr, const int *__restrict__ idx,
+                          const double *__restrict__ data, double *__restrict__ dense) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long m = 4 * n;
+    for (long long p = indptr[i]; p < indptr[i + 1]; ++p) {
+        const int j = idx[p];
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c) dense[(4 * i + r) * m + 4 * j + c] = data[p * 16 + r * 4 + c];
+    }
+}
+
+// Gauss-Jordan inverse of an m x m matrix (m <= 128) in shared memory by one CTA, partial
+// pivoting; ok[0] = 0 if a pivot vanishes
+__global__ void k_dense_inverse(int m, const double *__restrict__ A, double *__restrict__ inv,
+                                int *__restrict__ ok) {
+    extern __shared__ double sm[];
+    double *a = sm;                 // m x m
+    double *e = sm + m * m;         // m x m, the inverse being built
+    __shared__ int piv;
+    __shared__ int bad;
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+        a[t] = A[t];
+        e[t] = (t / m == t % m) ? 1.0 : 0.0;
+    }
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int k = 0; k < m; ++k) {
+        if (threadIdx.x == 0) {
+            int p = k;
+            double best = fabs(a[k * m + k]);
+            for (int r = k + 1; r < m; ++r)
+                if (fabs(a[r * m + k]) > best) { best = fabs(a[r * m + k]); p = r; }
+            piv = p;
+            if (!(best > 0.0)) bad = 1;
+        }
+        __syncthreads();
+        if (bad) break;
+        const int p = piv;
+        if (p != k)
+            for (int c = threadIdx.x; c < m; c += blockDim.x) {
+                double t = a[k * m + c]; a[k * m + c] = a[p * m + c]; a[p * m + c] = t;
+                t = e[k * m + c]; e[k * m + c] = e[p * m + c]; e[p * m + c] = t;
+            }
+        __syncthreads();
+        const double d = 1.0 / a[k * m + k];
+        __syncthreads();
+        for (int c = threadIdx.x; c < m; c += blockDim.x) {
+            a[k * m + c] *= d;
+            e[k * m + c] *= d;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+            const int r = t / m, c = t % m;
+            if (r == k) continue;
+            const double f = a[r * m + k];
+            if (c != k) a[t] -= f * a[k * m + c];
+            e[t] -= f * e[k * m + c];
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < m; r += blockDim.x)
+            if (r != k) a[r * m + k] = 0.0;
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) inv[t] = e[t];
+    if (threadIdx.x == 0) *ok = bad ? 0 : 1;
+}
+
+// ------------------------------------------------------------------ V-cycle kernels
+
+// Damped block Jacobi: x_out = x_in + omega D^-1 (b - A x_in); FIRST: x_in = 0 (no product).
+// Lane layout of the SpMV (G lanes per row, 4-lane slots), then the four residual components
+// are gathered into each lane of slot 0 for the 4x4 inverse.
+template <int G, bool FIRST, typename V, typename T>
+__global__ void __launch_bounds__(256)
+k_jacobi(long long n, const long long *__restrict__ indptr, const int *__restrict__ indices,
+         const V *__restrict__ data, const V *__restrict__ dinv, const T *__restrict__ b,
+         const T *__restrict__ xin, T *__restrict__ xout, T omega) {
+    constexpr int S = G / 4;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = gid / G;
+    const int lane = threadIdx.x % G;
+    const int slot = lane / 4, r = lane % 4;
+    T acc = 0;
+    if (!FIRST && row < n) {
+        const long long p1 = indptr[row + 1];
+        for (long long p = indptr[row] + slot; p < p1; p += S) {
+            const int j = __ldcs(indices + p);
+            const Vec4<V> a = Vec4<V>::load_stream(data + p * 16 + r * 4);
+            const Vec4<T> xv = Vec4<T>::load(xin + (long long)j * 4);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc += (T)a.v[c] * xv.v[c];
+        }
+    }
+    if (!FIRST) {
+#pragma unroll
+        for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    }
+    T res = 0;
+    if (row < n) res = b[row * 4 + r] - acc;
+    // gather the row's 4 residual components (lanes 0..3 of the group hold them)
+    const int base = (threadIdx.x % 32) / G * G;
+    T rc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rc[c] = __shfl_sync(0xffffffffu, res, base + c);
+    if (row < n && slot == 0) {
+        const Vec4<V> d = Vec4<V>::load(dinv + row * 16 + r * 4);
+        T upd = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) upd += (T)d.v[c] * rc[c];
+        const T x0 = FIRST ? (T)0 : xin[row * 4 + r];
+        xout[row * 4 + r] = x0 + omega * upd;
+    }
+}
+
+// coarse residual: rc[I] = sum over the aggregate's members (ascending) of r[i]
+template <typename T>
+__global__ void k_restrict(long long nc, const long long *__restrict__ mptr, const int *__restrict__ mem,
+                           const T *__restrict__ r, T *__restrict__ rc) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc * 4) return;
+    const long long I = t / 4;
+    const int c = (int)(t % 4);
+    T acc = 0;
+    for (long long q = mptr[I]; q < mptr[I + 1]; ++q) acc += r[(long long)mem[q] * 4 + c];
+    rc[t] = acc;
+}
+
+template <typename T>
+__global__ void k_prolong_add(long long n, const int *__restrict__ agg, const T *__restrict__ e,
+                              T *__restrict__ x) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * 4) return;
+    const long long i = t / 4;
+    x[t] += e[(long long)agg[i] * 4 + (t % 4)];
+}
+
+// x = inv b for a dense coarsest level (m x m), one warp per output row
+template <typename V, typename T>
+__global__ void k_dense_apply(int m, const V *__restrict__ inv, const T *__restrict__ b, T *__restrict__ x) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (row >= m) return;
+    T acc = 0;
+    for (int c = lane; c < m; c += 32) acc += (T)inv[(long long)row * m + c] * b[c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) x[row] = acc;
+}
+
+// ------------------------------------------------------------------ host-side structures
+
+struct Level {
+    long long n = 0, nnz = 0;
+    const long long *indptr = nullptr;
+    const int *indices = nullptr;
+    const double *data = nullptr;         // FP64 blocks (level 0: the caller's matrix)
+    long long *dpos = nullptr;
+    long long *rows = nullptr;            // row of every entry
+    double *dinv64 = nullptr;
+    float *data32 = nullptr, *dinv32 = nullptr;
+    int lanes = 8;
+    // transfer to the next level (kept while the aggregation is kept)
+    int *agg = nullptr;
+    long long nc = 0;
+    long long *mptr = nullptr;
+    int *mem = nullptr;
+    long long *gperm = nullptr, *gseg = nullptr;   // Galerkin: fine blocks by coarse key
+    long long cnnz = 0;
+    // dense coarsest
+    bool dense = false;
+    double *inv64 = nullptr;
+    float *inv32 = nullptr;
+    // cycle vectors
+    void *x = nullptr, *x2 = nullptr, *b = nullptr, *r = nullptr;
+};
+
+struct Params {
+    int precision = 0;       // 0 FP64 cycle, 1 FP32 cycle
+    int strength = 0;        // 0 block norm, 1 pressure-pressure entry
+    int passes = 2;
+    int presweeps = 2, postsweeps = 2;
+    double omega = 0.7;
+    int coarse_sweeps = 8;
+    int max_levels = 25;
+    int rebuild_every = 10;
+};
+
+inline int lanes_for(long long n, long long nnz) {
+    const double per = n ? (double)nnz / n : 0.0;
+    return per > 40 ? 32 : (per > 12 ? 16 : 8);
+}
+
+}  // namespace amg
+}  // namespace zvfv

@@ -1,0 +1,891 @@
+// The linear back end: FGMRES (right-preconditioned, flexible) around the aggregation
+// multigrid of amg.cuh, behind an opaque handle in the manner of the reference's AmgX binding
+// (zvcfd/fv/linear.py:681-955): create, set up for a matrix (structure on the first call,
+// coefficients later), solve, one V-cycle, destroy.
+//
+// FGMRES follows zvcfd/fv/linear.py:172-320: restart length `restart`, classical Gram-Schmidt
+// with one reorthogonalisation pass (CGS2), convergence when the residual has fallen by
+// `rtol` relative to the initial one or to round-off (1e-13 ||b||), and the rank-one terms
+// u w^T of lumped outlets applied in every product. The Arnoldi step runs in three fused
+// passes over the basis (dots; update + dots; update + norm) with deterministic two-stage
+// reductions, and the Hessenberg matrix, its Givens rotations and the residual estimate stay
+// on the device: the host reads 3 numbers per Krylov step.
+#include <cmath>
+#include <vector>
+
+#include "amg.cuh"
+
+namespace zvfv {
+
+using namespace amg;
+
+namespace {
+
+constexpr int MAXV = 32;         // basis vectors per reduction (restart + 1 <= 32)
+constexpr int DOT_THREADS = 256;
+
+__device__ inline double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// partial[cta][j] = sum over the CTA's rows of V[j][i] * w[i], j < nv (MODE 0)
+// MODE 1: w -= sum_j h[j] V[j] first, then the dots with the updated w
+// MODE 2: w -= sum_j h[j] V[j], then partial[cta][0] = ||w||^2
+template <int MODE>
+__global__ void __launch_bounds__(DOT_THREADS)
+k_arnoldi_pass(long long n, const double *__restrict__ V, long long ldv, int nv,
+               const double *__restrict__ h, double *__restrict__ w, double *__restrict__ partial) {
+    double acc[MAXV];
+#pragma unroll
+    for (int j = 0; j < MAXV; ++j) acc[j] = 0.0;
+    __shared__ double hs[MAXV];
+    if (MODE > 0 && threadIdx.x < MAXV) hs[threadIdx.x] = threadIdx.x < nv ? h[threadIdx.x] : 0.0;
+    __syncthreads();
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double wi = w[i];
+        if (MODE > 0) {
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < MAXV; ++j)
+                if (j < nv) s += hs[j] * V[j * ldv + i];
+            wi -= s;
+            w[i] = wi;
+        }
+        if (MODE < 2) {
+#pragma unroll
+            for (int j = 0; j < MAXV; ++j)
+                if (j < nv) acc[j] += V[j * ldv + i] * wi;
+        } else {
+            acc[0] += wi * wi;
+        }
+    }
+    __shared__ double red[DOT_THREADS / 32][MAXV];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int cols = MODE < 2 ? nv : 1;
+#pragma unroll
+    for (int j = 0; j < MAXV; ++j)
+        if (j < cols) {
+            const double v = warp_sum(acc[j]);
+            if (lane == 0) red[warp][j] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < cols) {
+        double v = 0.0;
+        for (int q = 0; q < DOT_THREADS / 32; ++q) v += red[q][threadIdx.x];
+        partial[(long long)blockIdx.x * MAXV + threadIdx.x] = v;
+    }
+}
+
+// out[j] = sum over CTAs (in order) of partial[cta][j]
+__global__ void k_fold_cols(int ncta, int cols, const double *__restrict__ partial, double *__restrict__ out) {
+    const int j = threadIdx.x;
+    if (j >= cols) return;
+    double v = 0.0;
+    for (int c = 0; c < ncta; ++c) v += partial[(long long)c * MAXV + j];
+    out[j] = v;
+}
+
+// partial dots of two vectors (a . b), MAXV-strided partials in column 0
+__global__ void __launch_bounds__(DOT_THREADS)
+k_dot_partial(long long n, const double *__restrict__ a, const double *__restrict__ b,
+              double *__restrict__ partial) {
+    double acc = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        acc += a[i] * b[i];
+    __shared__ double red[DOT_THREADS / 32];
+    acc = warp_sum(acc);
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int q = 0; q < DOT_THREADS / 32; ++q) v += red[q];
+        partial[(long long)blockIdx.x * MAXV] = v;
+    }
+}
+
+// Column k of the Hessenberg matrix from the two Gram-Schmidt passes and ||w||, the earlier
+// Givens rotations applied, a new one formed, the residual estimate updated.
+// st: [0] |g[k+1]|, [1] h_{k+1,k}, [2] 1/h_{k+1,k} (0 if it vanished)
+__global__ void k_arnoldi_finish(int k, int ldh, const double *__restrict__ h1,
+                                 const double *__restrict__ h2, const double *__restrict__ nrm2,
+                                 double *__restrict__ H, double *__restrict__ cs, double *__restrict__ sn,
+                                 double *__restrict__ g, double *__restrict__ st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double *col = H + (long long)k * ldh;          // column k, rows 0..k+1
+    for (int j = 0; j <= k; ++j) col[j] = h1[j] + h2[j];
+    const double hn = sqrt(nrm2[0]);
+    col[k + 1] = hn;
+    for (int j = 0; j < k; ++j) {
+        const double t = cs[j] * col[j] + sn[j] * col[j + 1];
+        col[j + 1] = -sn[j] * col[j] + cs[j] * col[j + 1];
+        col[j] = t;
+    }
+    const double den = hypot(col[k], col[k + 1]);
+    if (den != 0.0) {
+        cs[k] = col[k] / den;
+        sn[k] = col[k + 1] / den;
+    } else {
+        cs[k] = 1.0;
+        sn[k] = 0.0;
+    }
+    col[k] = den;
+    col[k + 1] = 0.0;
+    g[k + 1] = -sn[k] * g[k];
+    g[k] = cs[k] * g[k];
+    st[0] = fabs(g[k + 1]);
+    st[1] = hn;
+    st[2] = hn != 0.0 ? 1.0 / hn : 0.0;
+}
+
+__global__ void k_init_g(int m, double beta, double *__restrict__ g) {
+    const int i = threadIdx.x;
+    if (i <= m) g[i] = i == 0 ? beta : 0.0;
+}
+
+// y = H(0:kk, 0:kk)^-1 g (upper triangular)
+__global__ void k_upper_solve(int kk, int ldh, const double *__restrict__ H, const double *__restrict__ g,
+                              double *__restrict__ y) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = kk - 1; i >= 0; --i) {
+        double s = g[i];
+        for (int j = i + 1; j < kk; ++j) s -= H[(long long)j * ldh + i] * y[j];
+        y[i] = s / H[(long long)i * ldh + i];
+    }
+}
+
+// x += sum_j y[j] Z[j]
+__global__ void k_combine(long long n, const double *__restrict__ Z, long long ldz, int kk,
+                          const double *__restrict__ y, double *__restrict__ x) {
+    __shared__ double ys[MAXV];
+    if (threadIdx.x < MAXV) ys[threadIdx.x] = threadIdx.x < kk ? y[threadIdx.x] : 0.0;
+    __syncthreads();
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < MAXV; ++j)
+            if (j < kk) s += ys[j] * Z[j * ldz + i];
+        x[i] += s;
+    }
+}
+
+// out = a * scale (host scalar) or a * scale_dev[0] (device scalar)
+__global__ void k_scale(long long n, const double *__restrict__ a, double scale,
+                        const double *__restrict__ scale_dev, double *__restrict__ out) {
+    const double s = scale_dev ? scale_dev[0] : scale;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = a[i] * s;
+}
+
+// rank-one terms: t = w . x over (wi, wv); y[ui] += sign * uv * t
+__global__ void k_lr_dot(long long m, const long long *__restrict__ wi, const double *__restrict__ wv,
+                         const double *__restrict__ x, double *__restrict__ t) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (long long q = threadIdx.x; q < m; q += blockDim.x) acc += wv[q] * x[wi[q]];
+    acc = warp_sum(acc);
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int q = 0; q < (int)(blockDim.x / 32); ++q) v += red[q];
+        t[0] = v;
+    }
+}
+
+__global__ void k_lr_axpy(long long m, const long long *__restrict__ ui, const double *__restrict__ uv,
+                          const double *__restrict__ t, double sign, double *__restrict__ y) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < m) y[ui[q]] += sign * uv[q] * t[0];
+}
+
+struct LowRank {
+    const long long *ui;
+    const double *uv;
+    long long nu;
+    const long long *wi;
+    const double *wv;
+    long long nw;
+};
+
+// ------------------------------------------------------------------ the hierarchy
+
+class Hierarchy {
+   public:
+    Params prm;
+    std::vector<Level> L;
+    int setups = 0;
+    cudaStream_t st = 0;
+    Arena structure, values, scratch;
+    const long long *src_indptr = nullptr;
+    long long src_n = -1, src_nnz = -1;
+
+    int setup(long long n, long long nnz, const long long *indptr, const int *indices,
+              const double *data, cudaStream_t s) {
+        st = s;
+        structure.set_stream(s);
+        values.set_stream(s);
+        scratch.set_stream(s);
+        const bool same = L.size() && n == src_n && nnz == src_nnz && indptr == src_indptr;
+        const bool rebuild = !same || prm.rebuild_every <= 1 || setups % prm.rebuild_every == 0;
+        ++setups;
+        values.release();
+        if (rebuild) {
+            structure.release();
+            L.clear();
+            Level l0;
+            l0.n = n;
+            l0.nnz = nnz;
+            l0.indptr = indptr;
+            l0.indices = indices;
+            l0.data = data;
+            L.push_back(l0);
+            src_indptr = indptr;
+            src_n = n;
+            src_nnz = nnz;
+            ZV_TRY(build_structure());
+        } else {
+            L[0].data = data;
+            L[0].indices = indices;
+        }
+        return build_values();
+    }
+
+    template <typename T>
+    int vcycle(const T *b0, T *x0);   // defined below
+
+   private:
+    // ---------------------------------------------------------------- sorting helpers
+
+    // keys (m) -> stable order perm, unique keys, segment starts (nseg + 1)
+    int sort_segments(Arena &out, const unsigned long long *keys, long long m, int end_bit,
+                      long long **perm, unsigned long long **ukeys, long long **seg, long long *nseg) {
+        unsigned long long *kout;
+        long long *idx;
+        int *flags, *rank;
+        ZV_TRY(scratch.get(&kout, m));
+        ZV_TRY(scratch.get(&idx, m));
+        ZV_TRY(out.get(perm, m));
+        ZV_TRY(scratch.get(&flags, m));
+        ZV_TRY(scratch.get(&rank, m));
+        k_iota64<<<grid_for(m, 256), 256, 0, st>>>(idx, m); count_launch();
+        size_t tb = 0, tb2 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, kout, idx, *perm, (int64_t)m, 0, end_bit, st);
+        cub::DeviceScan::ExclusiveSum(nullptr, tb2, flags, rank, (int64_t)m, st);
+        unsigned char *tmp;
+        ZV_TRY(scratch.get(&tmp, tb > tb2 ? tb : tb2));
+        ZV_TRY(cuda_status(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, kout, idx, *perm, (int64_t)m, 0,
+                                                           end_bit, st), "sort"));
+        k_seg_flags<<<grid_for(m, 256), 256, 0, st>>>(m, kout, flags); count_launch();
+        ZV_TRY(cuda_status(cub::DeviceScan::ExclusiveSum(tmp, tb2, flags, rank, (int64_t)m, st), "scan"));
+        int last[2];
+        cudaMemcpyAsync(&last[0], rank + m - 1, 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last[1], flags + m - 1, 4, cudaMemcpyDeviceToHost, st);
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "segments"));
+        *nseg = (long long)last[0] + last[1];
+        ZV_TRY(out.get(seg, *nseg + 1));
+        ZV_TRY(out.get(ukeys, *nseg));
+        k_seg_starts<<<grid_for(m, 256), 256, 0, st>>>(m, flags, rank, kout, *seg, *ukeys); count_launch();
+        k_seg_end<<<1, 1, 0, st>>>(m, *nseg, *seg); count_launch();
+        return launch_status("segments");
+    }
+
+    int exclusive_scan(const int *in, int *out, long long n) {
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, (int64_t)n, st);
+        unsigned char *tmp;
+        ZV_TRY(scratch.get(&tmp, tb));
+        return cuda_status(cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, (int64_t)n, st), "scan");
+    }
+
+    static int bits(unsigned long long v) {
+        int b = 1;
+        while (b < 64 && (v >> b)) ++b;
+        return b;
+    }
+
+    // ---------------------------------------------------------------- aggregation
+
+    // pairwise matching on graph (n, indptr, idx) with strengths s (linear.py:373-413)
+    int pairwise(long long n, const long long *indptr, const int *idx, const double *s, int *agg,
+                 long long *count) {
+        int *best, *flag, *rank, *join, *nxt, *any;
+        ZV_TRY(scratch.get(&best, n));
+        ZV_TRY(scratch.get(&flag, n));
+        ZV_TRY(scratch.get(&rank, n));
+        ZV_TRY(scratch.get(&join, n));
+        ZV_TRY(scratch.get(&nxt, 1));
+        ZV_TRY(scratch.get(&any, 1));
+        const unsigned g = grid_for(n, 256);
+        k_fill_int<<<g, 256, 0, st>>>(agg, n, -1); count_launch();
+        cudaMemsetAsync(nxt, 0, 4, st);
+        for (int round = 0; round < 4; ++round) {
+            k_best_free<<<g, 256, 0, st>>>(n, indptr, idx, s, agg, best, any); count_launch();
+            k_leaders<<<g, 256, 0, st>>>(n, best, flag); count_launch();
+            ZV_TRY(exclusive_scan(flag, rank, n));
+            k_assign_pairs<<<g, 256, 0, st>>>(n, best, flag, rank, nxt, agg); count_launch();
+            k_advance<<<1, 1, 0, st>>>(flag, rank, n, nxt); count_launch();
+        }
+        k_join<<<g, 256, 0, st>>>(n, indptr, idx, s, agg, join); count_launch();
+        k_apply_join<<<g, 256, 0, st>>>(n, join, agg, flag); count_launch();
+        ZV_TRY(exclusive_scan(flag, rank, n));
+        k_assign_singles<<<g, 256, 0, st>>>(n, flag, rank, nxt, agg); count_launch();
+        k_advance<<<1, 1, 0, st>>>(flag, rank, n, nxt); count_launch();
+        int c = 0;
+        cudaMemcpyAsync(&c, nxt, 4, cudaMemcpyDeviceToHost, st);
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "pairwise"));
+        *count = c;
+        return launch_status("pairwise");
+    }
+
+    // `passes` pairwise passes (linear.py:415-433) -> agg (n), nc
+    int aggregate(Level &v) {
+        const long long n = v.n;
+        double *w;
+        ZV_TRY(scratch.get(&w, v.nnz));
+        k_block_weight<<<grid_for(v.nnz, 256), 256, 0, st>>>(v.nnz, v.data, prm.strength, w); count_launch();
+        long long gn = n, gnnz = v.nnz;
+        const long long *gptr = v.indptr;
+        const int *gidx = v.indices;
+        const long long *grows = v.rows;
+        const double *gw = w;
+        int *total;
+        ZV_TRY(structure.get(&total, n));
+        k_iota_int(total, n);
+        long long count = n;
+        for (int pass = 0; pass < prm.passes; ++pass) {
+            double *dw, *s;
+            int *a;
+            ZV_TRY(scratch.get(&dw, gn));
+            ZV_TRY(scratch.get(&s, gnnz));
+            ZV_TRY(scratch.get(&a, gn));
+            k_diag_of<<<grid_for(gn, 256), 256, 0, st>>>(gn, gptr, gidx, gw, dw, nullptr); count_launch();
+            k_strength<<<grid_for(gnnz, 256), 256, 0, st>>>(gnnz, grows, gidx, gw, dw, s); count_launch();
+            ZV_TRY(pairwise(gn, gptr, gidx, s, a, &count));
+            k_compose<<<grid_for(n, 256), 256, 0, st>>>(n, a, total); count_launch();
+            if (pass + 1 == prm.passes) break;
+            // the graph of the aggregates: strengths summed per aggregate pair
+            unsigned long long *keys, *ukeys;
+            long long *perm, *seg, nseg;
+            ZV_TRY(scratch.get(&keys, gnnz));
+            k_pair_key<<<grid_for(gnnz, 256), 256, 0, st>>>(gnnz, grows, gidx, a,
+                                                            (unsigned long long)count, keys); count_launch();
+            ZV_TRY(sort_segments(scratch, keys, gnnz, bits((unsigned long long)count * count), &perm,
+                                 &ukeys, &seg, &nseg));
+            long long *nptr, *nrows;
+            int *nidx;
+            double *nw;
+            ZV_TRY(scratch.get(&nptr, count + 1));
+            ZV_TRY(scratch.get(&nidx, nseg));
+            ZV_TRY(scratch.get(&nw, nseg));
+            ZV_TRY(scratch.get(&nrows, nseg));
+            k_keys_to_csr<<<grid_for((nseg > count ? nseg : count) + 1, 256), 256, 0, st>>>(
+                nseg, count, (unsigned long long)count, ukeys, nptr, nidx); count_launch();
+            k_seg_sum<<<grid_for(nseg, 256), 256, 0, st>>>(nseg, 1, seg, perm, gw, nw); count_launch();
+            k_rows_of<<<grid_for(count, 256), 256, 0, st>>>(count, nptr, nrows); count_launch();
+            gn = count;
+            gnnz = nseg;
+            gptr = nptr;
+            gidx = nidx;
+            grows = nrows;
+            gw = nw;
+        }
+        v.agg = total;
+        v.nc = count;
+        return launch_status("aggregate");
+    }
+
+    void k_iota_int(int *p, long long n) {
+        k_iota_i32_launch(p, n);
+    }
+    void k_iota_i32_launch(int *p, long long n);
+
+    int build_structure() {
+        for (size_t l = 0;; ++l) {
+            Level &v = L[l];
+            v.lanes = lanes_for(v.n, v.nnz);
+            ZV_TRY(structure.get(&v.dpos, v.n));
+            ZV_TRY(structure.get(&v.rows, v.nnz));
+            k_diag_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.indices, nullptr, nullptr,
+                                                          v.dpos); count_launch();
+            k_rows_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.rows); count_launch();
+            if (v.n <= DENSE_MAX) {
+                v.dense = true;
+                break;
+            }
+            if ((int)l + 1 >= prm.max_levels) break;
+            ZV_TRY(aggregate(v));
+            scratch.release();
+            if (v.nc >= 0.9 * v.n || v.nc < 1) {          // coarsening stalled: last level
+                v.agg = nullptr;
+                break;
+            }
+            // members of each aggregate, ascending (restriction)
+            unsigned long long *keys, *ukeys;
+            long long nseg;
+            ZV_TRY(scratch.get(&keys, v.n));
+            k_agg_keys(v.agg, v.n, keys);
+            long long *perm, *seg;
+            ZV_TRY(sort_segments(structure, keys, v.n, bits((unsigned long long)v.nc), &perm, &ukeys,
+                                 &seg, &nseg));
+            int *mem;
+            ZV_TRY(structure.get(&mem, v.n));
+            k_narrow(perm, v.n, mem);
+            v.mem = mem;
+            v.mptr = seg;
+            // the Galerkin map: fine blocks grouped by (agg row, agg col)
+            unsigned long long *gk;
+            ZV_TRY(scratch.get(&gk, v.nnz));
+            k_pair_key<<<grid_for(v.nnz, 256), 256, 0, st>>>(v.nnz, v.rows, v.indices, v.agg,
+                                                             (unsigned long long)v.nc, gk); count_launch();
+            unsigned long long *gu;
+            long long cn;
+            ZV_TRY(sort_segments(structure, gk, v.nnz, bits((unsigned long long)v.nc * v.nc), &v.gperm,
+                                 &gu, &v.gseg, &cn));
+            v.cnnz = cn;
+            long long *cptr;
+            int *cidx;
+            ZV_TRY(structure.get(&cptr, v.nc + 1));
+            ZV_TRY(structure.get(&cidx, cn));
+            k_keys_to_csr<<<grid_for((cn > v.nc ? cn : v.nc) + 1, 256), 256, 0, st>>>(
+                cn, v.nc, (unsigned long long)v.nc, gu, cptr, cidx); count_launch();
+            scratch.release();
+            Level c;
+            c.n = v.nc;
+            c.nnz = cn;
+            c.indptr = cptr;
+            c.indices = cidx;
+            L.push_back(c);
+        }
+        return launch_status("hierarchy structure");
+    }
+
+    void k_agg_keys(const int *agg, long long n, unsigned long long *keys);
+    void k_narrow(const long long *src, long long n, int *dst);
+
+    int build_values() {
+        for (size_t l = 0; l < L.size(); ++l) {
+            Level &v = L[l];
+            if (l > 0) {
+                const Level &f = L[l - 1];
+                double *d;
+                ZV_TRY(values.get(&d, v.nnz * 16));
+                k_seg_sum<<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz, 16, f.gseg, f.gperm, f.data, d); count_launch();
+                v.data = d;
+            }
+            ZV_TRY(values.get(&v.dinv64, v.n * 16));
+            k_dinv<double><<<grid_for(v.n, 128), 128, 0, st>>>(v.n, v.data, v.dpos, v.dinv64); count_launch();
+            if (prm.precision == 1) {
+                ZV_TRY(values.get(&v.data32, v.nnz * 16));
+                ZV_TRY(values.get(&v.dinv32, v.n * 16));
+                k_convert<double, float><<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz * 16, v.data, v.data32); count_launch();
+                k_convert<double, float><<<grid_for(v.n * 16, 256), 256, 0, st>>>(v.n * 16, v.dinv64, v.dinv32); count_launch();
+            }
+            if (v.dense) {
+                const int m = (int)(4 * v.n);
+                double *dense;
+                int *ok;
+                ZV_TRY(scratch.get(&dense, (size_t)m * m));
+                ZV_TRY(scratch.get(&ok, 1));
+                ZV_TRY(values.get(&v.inv64, (size_t)m * m));
+                cudaMemsetAsync(dense, 0, sizeof(double) * m * m, st);
+                k_densify<<<grid_for(v.n, 64), 64, 0, st>>>(v.n, v.indptr, v.indices, v.data, dense); count_launch();
+                const size_t smem = sizeof(double) * 2 * m * m;
+                cudaFuncSetAttribute(k_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                k_dense_inverse<<<1, 512, smem, st>>>(m, dense, v.inv64, ok); count_launch();
+                int okh = 0;
+                cudaMemcpyAsync(&okh, ok, 4, cudaMemcpyDeviceToHost, st);
+                ZV_TRY(cuda_status(cudaStreamSynchronize(st), "coarse inverse"));
+                if (!okh) {
+                    v.dense = false;      // singular: smooth the coarsest level instead
+                } else if (prm.precision == 1) {
+                    ZV_TRY(values.get(&v.inv32, (size_t)m * m));
+                    k_convert<double, float><<<grid_for((long long)m * m, 256), 256, 0, st>>>((long long)m * m,
+                                                                                           v.inv64, v.inv32); count_launch();
+                }
+                scratch.release();
+            }
+            const size_t vs = prm.precision == 1 ? sizeof(float) : sizeof(double);
+            char *buf;
+            ZV_TRY(values.get(&buf, 4 * vs * v.n * 4));
+            v.x = buf;
+            v.x2 = buf + vs * v.n * 4;
+            v.b = buf + 2 * vs * v.n * 4;
+            v.r = buf + 3 * vs * v.n * 4;
+        }
+        return launch_status("hierarchy values");
+    }
+
+    template <typename T>
+    int cycle(size_t l);
+};
+
+__global__ void k_iota_i32(int *p, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = (int)i;
+}
+
+__global__ void k_agg_keys_kernel(const int *agg, long long n, unsigned long long *keys) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keys[i] = (unsigned long long)agg[i];
+}
+
+__global__ void k_narrow_kernel(const long long *src, long long n, int *dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (int)src[i];
+}
+
+void Hierarchy::k_iota_i32_launch(int *p, long long n) {
+    k_iota_i32<<<grid_for(n, 256), 256, 0, st>>>(p, n); count_launch();
+}
+void Hierarchy::k_agg_keys(const int *agg, long long n, unsigned long long *keys) {
+    k_agg_keys_kernel<<<grid_for(n, 256), 256, 0, st>>>(agg, n, keys); count_launch();
+}
+void Hierarchy::k_narrow(const long long *src, long long n, int *dst) {
+    k_narrow_kernel<<<grid_for(n, 256), 256, 0, st>>>(src, n, dst); count_launch();
+}
+
+template <bool FIRST, typename V, typename T>
+void jacobi(int lanes, long long n, const long long *indptr, const int *indices, const V *data,
+            const V *dinv, const T *b, const T *xin, T *xout, T omega, cudaStream_t st) {
+    switch (lanes) {
+        case 8:
+            k_jacobi<8, FIRST, V, T><<<grid_for(n * 8, 256), 256, 0, st>>>(n, indptr, indices, data, dinv, b,
+                                                                         xin, xout, omega); count_launch();
+            break;
+        case 16:
+            k_jacobi<16, FIRST, V, T><<<grid_for(n * 16, 256), 256, 0, st>>>(n, indptr, indices, data, dinv,
+                                                                           b, xin, xout, omega); count_launch();
+            break;
+        default:
+            k_jacobi<32, FIRST, V, T><<<grid_for(n * 32, 256), 256, 0, st>>>(n, indptr, indices, data, dinv,
+                                                                           b, xin, xout, omega); count_launch();
+    }
+}
+
+template <typename T>
+struct CyclePick;
+template <>
+struct CyclePick<double> {
+    static const double *data(const Level &v) { return v.data; }
+    static const double *dinv(const Level &v) { return v.dinv64; }
+    static const double *inv(const Level &v) { return v.inv64; }
+};
+template <>
+struct CyclePick<float> {
+    static const float *data(const Level &v) { return v.data32; }
+    static const float *dinv(const Level &v) { return v.dinv32; }
+    static const float *inv(const Level &v) { return v.inv32; }
+};
+
+// one V-cycle on level l: L[l].b -> L[l].x (zero initial guess)
+template <typename T>
+int Hierarchy::cycle(size_t l) {
+    Level &v = L[l];
+    T *b = static_cast<T *>(v.b);
+    if (v.dense) {
+        const int m = (int)(4 * v.n);
+        k_dense_apply<T, T><<<grid_for((long long)m * 32, 256), 256, 0, st>>>(
+            m, CyclePick<T>::inv(v), b, static_cast<T *>(v.x)); count_launch();
+        return OK;
+    }
+    const auto *data = CyclePick<T>::data(v);
+    const auto *dinv = CyclePick<T>::dinv(v);
+    const T omega = (T)prm.omega;
+    const bool last = (l + 1 == L.size()) || v.agg == nullptr;
+    const int pre = last ? prm.coarse_sweeps : prm.presweeps;
+    jacobi<true>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, (const T *)nullptr,
+                 static_cast<T *>(v.x), omega, st);
+    for (int s = 1; s < pre; ++s) {
+        jacobi<false>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, static_cast<const T *>(v.x),
+                      static_cast<T *>(v.x2), omega, st);
+        std::swap(v.x, v.x2);
+    }
+    if (last) return launch_status("coarse smoothing");
+    T *r = static_cast<T *>(v.r);
+    ZV_TRY(bsr_spmv_launch<true, typename std::remove_const<typename std::remove_pointer<decltype(data)>::type>::type, T>(
+        v.lanes, v.n, v.indptr, v.indices, data, static_cast<const T *>(v.x), b, r, st));
+    Level &c = L[l + 1];
+    k_restrict<T><<<grid_for(c.n * 4, 256), 256, 0, st>>>(c.n, v.mptr, v.mem, r, static_cast<T *>(c.b)); count_launch();
+    ZV_TRY(cycle<T>(l + 1));
+    k_prolong_add<T><<<grid_for(v.n * 4, 256), 256, 0, st>>>(v.n, v.agg, static_cast<const T *>(c.x),
+                                                            static_cast<T *>(v.x)); count_launch();
+    for (int s = 0; s < prm.postsweeps; ++s) {
+        jacobi<false>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, static_cast<const T *>(v.x),
+                      static_cast<T *>(v.x2), omega, st);
+        std::swap(v.x, v.x2);
+    }
+    return launch_status("v-cycle");
+}
+
+// ------------------------------------------------------------------ the solver handle
+
+struct Solver {
+    Hierarchy H;
+    int restart = 30;
+    int lanes0 = 8;
+    cudaStream_t st = 0;
+    Arena work;
+    long long n4 = 0;
+    double *V = nullptr, *Z = nullptr, *w = nullptr, *r = nullptr, *x = nullptr;
+    double *Hm = nullptr, *cs = nullptr, *sn = nullptr, *g = nullptr, *y = nullptr;
+    double *h1 = nullptr, *h2 = nullptr, *nrm = nullptr, *stat = nullptr, *partial = nullptr;
+    double *lr_t = nullptr;
+    double *host = nullptr;        // pinned: 4 doubles
+    int ncta = 0;
+    long long n = 0, nnz = 0;
+    const long long *indptr = nullptr;
+    const int *indices = nullptr;
+    const double *data = nullptr;
+
+    ~Solver() {
+        if (host) cudaFreeHost(host);
+    }
+
+    int ensure_work(long long n4_) {
+        if (n4_ == n4 && V) return OK;
+        work.set_stream(st);
+        work.release();
+        n4 = n4_;
+        const int m = restart;
+        ZV_TRY(work.get(&V, (size_t)(m + 1) * n4));
+        ZV_TRY(work.get(&Z, (size_t)m * n4));
+        ZV_TRY(work.get(&w, n4));
+        ZV_TRY(work.get(&r, n4));
+        ZV_TRY(work.get(&x, n4));
+        ZV_TRY(work.get(&Hm, (size_t)(m + 1) * (m + 1)));
+        ZV_TRY(work.get(&cs, m + 1));
+        ZV_TRY(work.get(&sn, m + 1));
+        ZV_TRY(work.get(&g, m + 2));
+        ZV_TRY(work.get(&y, m + 1));
+        ZV_TRY(work.get(&h1, MAXV));
+        ZV_TRY(work.get(&h2, MAXV));
+        ZV_TRY(work.get(&nrm, MAXV));
+        ZV_TRY(work.get(&stat, 4));
+        ZV_TRY(work.get(&lr_t, 1));
+        ncta = (int)std::min<long long>(grid_for(n4, DOT_THREADS * 4), 4LL * sm_count());
+        ZV_TRY(work.get(&partial, (size_t)ncta * MAXV));
+        if (!host) ZV_TRY(cuda_status(cudaMallocHost((void **)&host, 8 * sizeof(double)), "pinned"));
+        return OK;
+    }
+
+    // y = A x (+ rank-one terms); resid: y = b - A x
+    int apply(const double *xin, const double *b, double *out, const std::vector<LowRank> &lr) {
+        if (b) ZV_TRY(bsr_spmv_launch<true, double, double>(lanes0, n, indptr, indices, data, xin, b, out, st));
+        else ZV_TRY(bsr_spmv_launch<false, double, double>(lanes0, n, indptr, indices, data, xin, nullptr, out, st));
+        for (const LowRank &t : lr) {
+            k_lr_dot<<<1, 256, 0, st>>>(t.nw, t.wi, t.wv, xin, lr_t); count_launch();
+            k_lr_axpy<<<grid_for(t.nu, 256), 256, 0, st>>>(t.nu, t.ui, t.uv, lr_t, b ? -1.0 : 1.0, out); count_launch();
+        }
+        return launch_status("operator");
+    }
+
+    int dot2(const double *a, const double *b, double *out_dev) {
+        k_dot_partial<<<ncta, DOT_THREADS, 0, st>>>(n4, a, b, partial); count_launch();
+        k_fold_cols<<<1, MAXV, 0, st>>>(ncta, 1, partial, out_dev); count_launch();
+        return launch_status("dot");
+    }
+
+    int precondition(const double *in, double *out) {
+        if (H.prm.precision == 1) {
+            Level &v0 = H.L[0];
+            k_convert<double, float><<<grid_for(n4, 256), 256, 0, st>>>(n4, in, static_cast<float *>(v0.b)); count_launch();
+            ZV_TRY(H.vcycle<float>(nullptr, nullptr));
+            k_convert<float, double><<<grid_for(n4, 256), 256, 0, st>>>(n4, static_cast<const float *>(v0.x), out); count_launch();
+        } else {
+            Level &v0 = H.L[0];
+            cudaMemcpyAsync(v0.b, in, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+            ZV_TRY(H.vcycle<double>(nullptr, nullptr));
+            cudaMemcpyAsync(out, v0.x, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        }
+        return launch_status("precondition");
+    }
+
+    int solve(const double *b, double *xio, double rtol, int maxiter, const std::vector<LowRank> &lr,
+              int *iterations, double *residual, int *converged) {
+        const int m = restart;
+        const int ldh = m + 1;
+        cudaMemcpyAsync(x, xio, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        ZV_TRY(apply(x, b, r, lr));
+        ZV_TRY(dot2(b, b, nrm));
+        ZV_TRY(dot2(r, r, nrm + 1));
+        cudaMemcpyAsync(host, nrm, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "solve start"));
+        const double nb2 = host[0], nr2 = host[1];
+        double bnorm = std::sqrt(nr2);
+        if (bnorm == 0.0) bnorm = 1.0;
+        const double rt = std::max(rtol, 1e-13 * std::sqrt(nb2) / bnorm);
+        double beta = std::sqrt(nr2);
+        double res = beta / bnorm;
+        int it = 0;
+        while (res > rt && it < maxiter && std::isfinite(res)) {
+            k_scale<<<ncta, 256, 0, st>>>(n4, r, 1.0 / beta, nullptr, V); count_launch();
+            k_init_g<<<1, 64, 0, st>>>(m, beta, g); count_launch();
+            int kk = 0;
+            for (int k = 0; k < m; ++k) {
+                double *vk = V + (size_t)k * n4, *zk = Z + (size_t)k * n4;
+                ZV_TRY(precondition(vk, zk));
+                ZV_TRY(apply(zk, nullptr, w, lr));
+                const int nv = k + 1;
+                k_arnoldi_pass<0><<<ncta, DOT_THREADS, 0, st>>>(n4, V, n4, nv, nullptr, w, partial); count_launch();
+                k_fold_cols<<<1, MAXV, 0, st>>>(ncta, nv, partial, h1); count_launch();
+                k_arnoldi_pass<1><<<ncta, DOT_THREADS, 0, st>>>(n4, V, n4, nv, h1, w, partial); count_launch();
+                k_fold_cols<<<1, MAXV, 0, st>>>(ncta, nv, partial, h2); count_launch();
+                k_arnoldi_pass<2><<<ncta, DOT_THREADS, 0, st>>>(n4, V, n4, nv, h2, w, partial); count_launch();
+                k_fold_cols<<<1, MAXV, 0, st>>>(ncta, 1, partial, nrm); count_launch();
+                k_arnoldi_finish<<<1, 1, 0, st>>>(k, ldh, h1, h2, nrm, Hm, cs, sn, g, stat); count_launch();
+                ZV_TRY(launch_status("arnoldi"));
+                cudaMemcpyAsync(host, stat, 3 * sizeof(double), cudaMemcpyDeviceToHost, st);
+                ZV_TRY(cuda_status(cudaStreamSynchronize(st), "arnoldi step"));
+                ++it;
+                kk = k + 1;
+                res = host[0] / bnorm;
+                const double hn = host[1];
+                if (res <= rt || it >= maxiter || hn == 0.0 || !std::isfinite(res)) break;
+                k_scale<<<ncta, 256, 0, st>>>(n4, w, 0.0, stat + 2, V + (size_t)(k + 1) * n4); count_launch();
+            }
+            k_upper_solve<<<1, 1, 0, st>>>(kk, ldh, Hm, g, y); count_launch();
+            k_combine<<<ncta, 256, 0, st>>>(n4, Z, n4, kk, y, x); count_launch();
+            ZV_TRY(apply(x, b, r, lr));
+            ZV_TRY(dot2(r, r, nrm));
+            cudaMemcpyAsync(host, nrm, sizeof(double), cudaMemcpyDeviceToHost, st);
+            ZV_TRY(cuda_status(cudaStreamSynchronize(st), "restart"));
+            beta = std::sqrt(host[0]);
+            res = beta / bnorm;
+            if (!std::isfinite(res)) break;
+        }
+        cudaMemcpyAsync(xio, x, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        *iterations = it;
+        *residual = res;
+        *converged = res <= 1.01 * rt ? 1 : 0;
+        ZV_TRY(launch_status("fgmres"));
+        return std::isfinite(res) ? OK : NON_FINITE;
+    }
+};
+
+}  // namespace
+
+template <typename T>
+int Hierarchy::vcycle(const T *, T *) {
+    return cycle<T>(0);
+}
+
+}  // namespace zvfv
+
+using namespace zvfv;
+
+extern "C" {
+
+int zvfv_solver_create(void **handle, int precision, int strength, int passes, int presweeps,
+                       int postsweeps, double omega, int coarse_sweeps, int max_levels,
+                       int rebuild_every, int restart) {
+    if (!handle || precision < 0 || precision > 1 || restart < 1 || restart > MAXV - 1 || passes < 1 ||
+        presweeps < 1 || postsweeps < 0 || max_levels < 1) {
+        set_error("solver_create: bad arguments");
+        return BAD_ARGUMENT;
+    }
+    Solver *s = new Solver;
+    s->H.prm.precision = precision;
+    s->H.prm.strength = strength;
+    s->H.prm.passes = passes;
+    s->H.prm.presweeps = presweeps;
+    s->H.prm.postsweeps = postsweeps;
+    s->H.prm.omega = omega;
+    s->H.prm.coarse_sweeps = coarse_sweeps;
+    s->H.prm.max_levels = max_levels;
+    s->H.prm.rebuild_every = rebuild_every;
+    s->restart = restart;
+    *handle = s;
+    return OK;
+}
+
+int zvfv_solver_setup(void *handle, int64_t n, int64_t nnzb, const int64_t *indptr,
+                      const int32_t *indices, const double *data, void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || n <= 0 || nnzb <= 0) {
+        set_error("solver_setup: bad arguments");
+        return BAD_ARGUMENT;
+    }
+    s->st = as_stream(stream);
+    s->n = n;
+    s->nnz = nnzb;
+    s->indptr = (const long long *)indptr;
+    s->indices = indices;
+    s->data = data;
+    s->lanes0 = lanes_for(n, nnzb);
+    ZV_TRY(s->ensure_work(n * 4));
+    return s->H.setup(n, nnzb, (const long long *)indptr, indices, data, s->st);
+}
+
+int zvfv_solver_solve(void *handle, const double *b, double *x, double rtol, int maxiter,
+                      int n_lowrank, const int64_t *const *u_idx, const double *const *u_val,
+                      const int64_t *u_len, const int64_t *const *w_idx, const double *const *w_val,
+                      const int64_t *w_len, int *iterations, double *residual, int *converged,
+                      void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || !s->data || !b || !x || maxiter < 0) {
+        set_error("solver_solve: not set up or bad arguments");
+        return BAD_ARGUMENT;
+    }
+    s->st = as_stream(stream);
+    std::vector<LowRank> lr;
+    for (int q = 0; q < n_lowrank; ++q)
+        lr.push_back({(const long long *)u_idx[q], u_val[q], (long long)u_len[q],
+                      (const long long *)w_idx[q], w_val[q], (long long)w_len[q]});
+    return s->solve(b, x, rtol, maxiter, lr, iterations, residual, converged);
+}
+
+int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || !s->data) {
+        set_error("solver_vcycle: not set up");
+        return BAD_ARGUMENT;
+    }
+    s->st = as_stream(stream);
+    return s->precondition(r, z);
+}
+
+// levels, and per level rows and blocks (arrays of max_levels entries)
+int zvfv_solver_stats(void *handle, int max_levels, int *levels, int64_t *rows, int64_t *blocks) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s) return BAD_ARGUMENT;
+    *levels = (int)s->H.L.size();
+    for (int l = 0; l < *levels && l < max_levels; ++l) {
+        rows[l] = s->H.L[l].n;
+        blocks[l] = s->H.L[l].nnz;
+    }
+    return OK;
+}
+
+// level l's size, and its aggregate of every row (into agg, n entries, if not null)
+int zvfv_solver_level(void *handle, int level, int64_t *n, int64_t *nnzb, int64_t *n_coarse,
+                      int32_t *agg, void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || level < 0 || level >= (int)s->H.L.size()) {
+        set_error("solver_level: no level %d", level);
+        return BAD_ARGUMENT;
+    }
+    const Level &v = s->H.L[level];
+    *n = v.n;
+    *nnzb = v.nnz;
+    *n_coarse = v.agg ? v.nc : 0;
+    if (agg && v.agg)
+        return cuda_status(cudaMemcpyAsync(agg, v.agg, v.n * sizeof(int), cudaMemcpyDeviceToDevice,
+                                           as_stream(stream)), "copy");
+    return OK;
+}
+
+int zvfv_solver_destroy(void *handle) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s) return OK;
+    cudaStreamSynchronize(s->st);
+    delete s;
+    return OK;
+}
+
+}  // extern "C"

@@ -210,19 +210,34 @@ def _c_array(name: str, a: np.ndarray, ctype: str) -> str:
     else:
         body = ", ".join(str(int(v)) for v in a.reshape(-1))
     dims = "".join(f"[{d}]" for d in a.shape)
-    return f"    static constexpr {ctype} {name}{dims} = {{{body}}};"
+    return f"static __constant__ {ctype} {name}{dims} = {{{body}}};"
+
+
+_TABLES = (("EDGE", "edge", "int"), ("TRIS", "tris", "int"), ("WPT", "weights", "double"),
+           ("NIPF", "N_ip", "double"), ("DN", "dN_ip", "double"), ("IPS", "node_ips", "int"),
+           ("SGN", "node_sgn", "double"))
 
 
 def header_source() -> str:
-    """C++ source of ``topology_tables.h``: one ``Topo<K>`` specialisation per type."""
+    """CUDA source of ``topology_tables.h``.
+
+    Per type: the tables as ``__constant__`` arrays (``k<KIND>_<TABLE>``), and a
+    ``Topo<K>`` traits struct with the sizes as compile-time constants and
+    pointers to its tables, so kernels templated on the type can size their
+    shared memory and unroll their loops.
+    """
     out = ["// Generated by zvcfd_b200.topology.write_header(); do not edit.",
            "// Element tables of the median-dual discretisation (flux points, shape functions).",
            "#pragma once", "", "namespace zvfv {", "",
-           "enum Kind { TET = 0, PYRAMID = 1, WEDGE = 2, HEX = 3 };", "",
+           "enum Kind { TET = 0, PYRAMID = 1, WEDGE = 2, HEX = 3 };",
+           f"constexpr int MAXI = {MAX_IP_PER_NODE};", "",
            "template <int K> struct Topo;", ""]
-    for k, kind in enumerate(KINDS):
+    for kind in KINDS:
         t = tables(kind)
-        out.append(f"template <> struct Topo<{kind.upper()}> {{")
+        K = kind.upper()
+        for cname, attr, ctype in _TABLES:
+            out.append(_c_array(f"k{K}_{cname}", getattr(t, attr), ctype))
+        out.append(f"template <> struct Topo<{K}> {{")
         out.append(f"    static constexpr int N = {t.n};")
         out.append(f"    static constexpr int NIP = {t.n_ip};")
         out.append(f"    static constexpr int NPTS = {t.n_pts};")
@@ -230,13 +245,13 @@ def header_source() -> str:
         out.append(f"    static constexpr int NG = {t.n_grad};")
         out.append(f"    static constexpr int REC = {t.record_doubles};")
         out.append(f"    static constexpr int EPB = {epb(t.n)};")
-        out.append(_c_array("EDGE", t.edge, "int"))
-        out.append(_c_array("TRIS", t.tris, "int"))
-        out.append(_c_array("WPT", t.weights, "double"))
-        out.append(_c_array("NIP_", t.N_ip, "double"))
-        out.append(_c_array("DN", t.dN_ip, "double"))
-        out.append(_c_array("IPS", t.node_ips, "int"))
-        out.append(_c_array("SGN", t.node_sgn, "double"))
+        out.append(f"    __device__ static const int (*edge())[2] {{ return k{K}_EDGE; }}")
+        out.append(f"    __device__ static const int (*tris())[3] {{ return k{K}_TRIS; }}")
+        out.append(f"    __device__ static const double (*wpt())[{t.n}] {{ return k{K}_WPT; }}")
+        out.append(f"    __device__ static const double (*nip())[{t.n}] {{ return k{K}_NIPF; }}")
+        out.append(f"    __device__ static const double (*dn())[{t.n}][3] {{ return k{K}_DN; }}")
+        out.append(f"    __device__ static const int (*ips())[MAXI] {{ return k{K}_IPS; }}")
+        out.append(f"    __device__ static const double (*sgn())[MAXI] {{ return k{K}_SGN; }}")
         out.append("};")
         out.append("")
     out.append("}  // namespace zvfv")
