@@ -147,25 +147,38 @@ def spmv_roofline(solver, reps=20):
     return out, n, nnzb
 
 
+class CpuCase:
+    """The oracle's outer iteration (NumPy assembly + ACM-FGMRES to 0.1 + mass flows) on a
+    shorter tube of the same cross-section: the bounded CPU sample of the workload."""
+
+    def __init__(self, n_axial=8):
+        from oracle.fv import OracleSolver
+        from oracle.linear import ACM, fgmres
+
+        m, fl, bcs = make_case(n_axial)
+        self.n_nodes = m.n_nodes
+        s = self.s = OracleSolver(m, fl, bcs)
+
+        def lin(data, b, x0):
+            acm = ACM().setup(s.indptr, s.indices, data)
+            A = s.to_csr(data)
+            x, *_ = fgmres(lambda v: A @ v, b, x0, acm.vcycle, rtol=0.1, maxiter=200)
+            return x
+
+        self.lin = lin
+
+    def step(self) -> float:
+        t = time.perf_counter()
+        self.s.solve(max_iterations=1, tol=0.0, linear=self.lin, resume=True)
+        return time.perf_counter() - t
+
+
 def cpu_sample(n_axial=8, steps=1, warmup=1):
-    """The oracle's outer iteration (assembly + ACM-FGMRES to 0.1 + mass flows) on a shorter
-    tube of the same cross-section; returns seconds per outer iteration and the node count."""
-    from oracle.fv import OracleSolver
-    from oracle.linear import ACM, fgmres
-
-    m, fl, bcs = make_case(n_axial)
-    s = OracleSolver(m, fl, bcs)
-
-    def lin(data, b, x0):
-        acm = ACM().setup(s.indptr, s.indices, data)
-        A = s.to_csr(data)
-        x, *_ = fgmres(lambda v: A @ v, b, x0, acm.vcycle, rtol=0.1, maxiter=200)
-        return x
-
-    s.solve(max_iterations=warmup, tol=0.0, linear=lin)
-    t = time.perf_counter()
-    s.solve(max_iterations=steps, tol=0.0, linear=lin)
-    return (time.perf_counter() - t) / steps, m.n_nodes
+    """Seconds per oracle outer iteration on the short tube, and its node count."""
+    c = CpuCase(n_axial)
+    for _ in range(warmup):
+        c.step()
+    return float(np.mean([c.step() for _ in range(steps)])), c.n_nodes
 
 
 def cpu_spmv_gbs(indptr, indices, data, reps=3):
@@ -187,12 +200,11 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     full_nodes = 400686
-    times = []
-    n_nodes = None
-    for i in range(args.warmup + args.steps):
-        t, n_nodes = cpu_sample(n_axial=args.cpu_axial, steps=1, warmup=1 if i == 0 else 0)
-        if i >= args.warmup:
-            times.append(t)
+    c = CpuCase(args.cpu_axial)
+    for _ in range(args.warmup):
+        c.step()
+    times = [c.step() for _ in range(args.steps)]
+    n_nodes = c.n_nodes
     per = float(np.mean(times)) * full_nodes / n_nodes
     value = 1.0 / per
     sample = (f"oracle outer iteration (NumPy assembly + ACM-FGMRES to 0.1) on the same tube "
@@ -208,6 +220,15 @@ def reference_arm(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def max_over_ranks(value, dist, device):
+    """The largest of every rank's ``value`` (the job's time is its slowest replica's)."""
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_steps(solver, steps):
@@ -265,9 +286,7 @@ def main():
         elapsed, recs = run_steps(solver, args.steps)
     launches = lib.zvfv_launch_count() - l0
     if dist:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+        elapsed = max_over_ranks(elapsed, dist, "cuda")
         dist.barrier()
     per = elapsed / args.steps
     value = world * args.steps / elapsed

@@ -158,6 +158,15 @@ int zvfv_update(int64_t n, const double *x, double *U, double *P, double *partia
 int zvfv_fold(int64_t nrows, int width, const double *partial, const int32_t *ops, double *out,
               void *stream);
 
+/* Wall shear stress (N, 3) at wall nodes from the wall integration points of their sub-faces
+ * (WallGradientShear.__call__, zvcfd/fv/wall.py:107-137): node_ptr int64 (N+1) groups the
+ * ips by node; per ip the owning element's nodes elem int32 (M, 8, -1 padded), shape
+ * gradients grad (M, 8, 3), unit outward normal (M, 3) and area (M). */
+int zvfv_wall_shear(int64_t n_nodes, const int64_t *node_ptr, const int32_t *elem,
+                    const double *grad, const double *normal, const double *area,
+                    const double *U, int rheo, double mu0, double muinf, double lam, double ca,
+                    double cn, double *tau, void *stream);
+
 /* ---------------------------------------------------------------- block-CSR products */
 
 /* y = A x for 4x4 block CSR (kernel bsr_mv, zvcfd/fv/linear.py:47-61; BlockMatrix.matvec

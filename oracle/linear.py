@@ -136,7 +136,7 @@ class ACM:
     """Additive-correction multigrid on the CPU (``zvcfd/fv/linear.py:328-518``): pairwise
     aggregation, Galerkin block sums, damped block-Jacobi smoothing, a dense coarsest solve."""
 
-    def __init__(self, *, smooth=2, omega=0.7, coarse=32, passes=2, mode=0, max_levels=25,
+    def __init__(self, *, smooth=2, omega=0.7, coarse=24, passes=2, mode=0, max_levels=25,
                  coarse_sweeps=8):
         self.smooth, self.omega, self.coarse, self.passes = smooth, omega, coarse, passes
         self.mode, self.max_levels, self.coarse_sweeps = mode, max_levels, coarse_sweeps

@@ -103,3 +103,16 @@ def pipe_bcs(name: str, g: dict, m):
 
 
 PIPES = ("pipe_reference_tube", "pipe_tet_si", "curved_cy")
+
+
+def transient_bcs(g: dict, m):
+    R, umax = float(g["radius"]), float(g["umax"])
+    z = {zz.name: k for k, zz in m.zones.items()}
+
+    def prof(x, t):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+        amp = 1.0 + 0.5 * np.sin(2 * np.pi * t / 0.8)
+        return np.stack([0 * r2, 0 * r2, umax * amp * np.clip(1 - r2, 0, None)], 1)
+
+    return {z["inlet"]: {"kind": "velocity", "value": prof},
+            z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}

@@ -184,7 +184,57 @@ def pipe_cases() -> dict:
     return cases
 
 
+def transient_case() -> dict:
+    """The reference pipe marched 6 BDF2 steps from its steady state with a pulsatile inlet."""
+    R = 0.5
+    m = tube(R, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed", layers=1)
+    zid = {z.name: k for k, z in m.zones.items()}
+
+    def prof(x, t):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+        amp = 1.0 + 0.5 * np.sin(2 * np.pi * t / 0.8)
+        return np.stack([0 * r2, 0 * r2, 2 * amp * np.clip(1 - r2, 0, None)], 1)
+
+    bcs = {zid["inlet"]: {"kind": "velocity", "value": prof},
+           zid["outlet"]: {"kind": "pressure", "value": 0.0}, zid["wall"]: {"kind": "wall"}}
+    s = ReferenceSolver(m, Fluid(1.0, 0.2), bcs, advection=1.0, lag_rhie_chow=True)
+    rep = s.solve(max_iterations=400, tol=1e-12)
+    assert rep.converged
+    U0, P0 = s.U.copy(), s.P.copy()
+    s.solve_transient(0.05, 6, scheme="bdf2", loops=30, tol=1e-12)
+    return dict(mesh_arrays(m), U0=U0, P0=P0, U=s.U, P=s.P, rho=1.0, mu=0.2, radius=R, umax=2.0,
+                dt=0.05, steps=6, t_end=s.t)
+
+
+def wall_case() -> dict:
+    """The reference's wall shear stress (WallGradientShear) of two converged golden fields."""
+    from zvcfd.fv.wall import WallGradientShear
+
+    out = {}
+    for tag in ("pipe_reference_tube", "curved_cy"):
+        with np.load(HERE / f"{tag}.npz") as z:
+            g = {k: z[k] for k in z.files}
+        els = {k: g[f"elem_{k}"] for k in ("tet", "pyramid", "wedge", "hex") if f"elem_{k}" in g}
+        um = UnstructuredMesh(g["nodes"], els)
+        um.zones = {int(zid): BoundaryZone(int(zid), "", str(nm), g[f"zone_{int(zid)}"],
+                                           np.zeros(len(g[f"zone_{int(zid)}"]), np.int64))
+                    for zid, nm in zip(g["zone_ids"], g["zone_names"])}
+        wall = [int(zid) for zid, nm in zip(g["zone_ids"], g["zone_names"]) if str(nm) == "wall"]
+        op = WallGradientShear(um, wall)
+        visc = CarreauYasuda() if tag == "curved_cy" else None
+        out[f"{tag}_tau"] = op(g["U"], viscosity=visc, mu=float(g["mu"]))
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["wall"]:
+        np.savez_compressed(HERE / "wall_shear.npz", **wall_case())
+        print("wrote wall_shear")
+        return
+    if sys.argv[1:] == ["transient"]:
+        np.savez_compressed(HERE / "transient_pipe.npz", **transient_case())
+        print("wrote transient_pipe")
+        return
     tabs = {}
     for k in ("tet", "pyramid", "wedge", "hex"):
         t = topology(k)
@@ -199,6 +249,10 @@ def main():
     for tag, arrays in pipe_cases().items():
         np.savez_compressed(HERE / f"{tag}.npz", **arrays)
         print("wrote", tag, arrays["iterations"])
+    np.savez_compressed(HERE / "transient_pipe.npz", **transient_case())
+    print("wrote transient_pipe")
+    np.savez_compressed(HERE / "wall_shear.npz", **wall_case())
+    print("wrote wall_shear")
 
 
 if __name__ == "__main__":

@@ -1,0 +1,49 @@
+"""The host-side boundary data of the device path equal the oracle's (CPU)."""
+
+import numpy as np
+import pytest
+
+from fixtures import PIPES, fluid_of, load, mesh_of, pipe_bcs
+from oracle.fv import OracleSolver
+
+
+@pytest.mark.parametrize("name", PIPES)
+def test_boundary_arrays_match_oracle(name):
+    from zvcfd_b200.boundary import Boundary
+
+    g = load(name)
+    m = mesh_of(g)
+    bcs = pipe_bcs(name, g, m)
+    o = OracleSolver(m, fluid_of(g), bcs, advection=1.0)
+    b = Boundary(m, bcs, float(g["rho"]))
+    np.testing.assert_array_equal(b.vel_fixed_comp, o.vel_fixed_comp)
+    np.testing.assert_array_equal(b.p_fixed, o.p_fixed)
+    np.testing.assert_allclose(b.vel_value, o.vel_value, rtol=1e-15, atol=1e-300)
+    np.testing.assert_allclose(b.p_value, o.p_value)
+    np.testing.assert_allclose(b.inflow, o.inflow, rtol=1e-14, atol=1e-14 * np.abs(o.inflow).max())
+    np.testing.assert_allclose(b.pressure_area(), o._pressure_area(), rtol=1e-15)
+    np.testing.assert_allclose(b.inflow_offsets(), o.inflow_offsets(), atol=1e-15)
+    # the outlet force equals the oracle's outlet right-hand side for p = 0 (zero here)
+    force, a_out, w_cons, w_only, w_stab = b.outlet_arrays()
+    assert np.abs(force).max() == 0.0
+    tot = o._pressure_area()
+    assert np.all(w_cons[o.outlet] > 0) and np.all(w_cons[~o.outlet] == 0)
+    np.testing.assert_allclose(w_cons[o.outlet].sum(), (tot > 0).sum(), rtol=1e-12)
+    zids, W, c = b.flow_weights()
+    assert len(zids) == len(m.zones)
+
+
+def test_symmetry_and_pinned_pressure():
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.mesh import box
+
+    m = box((4, 3, 2), (3.0, 1.0, 0.5), kind="hex")
+    z = {zz.name: k for k, zz in m.zones.items()}
+    bcs = {z["xmin"]: {"kind": "velocity", "value": (1.0, 0.0, 0.0)},
+           z["xmax"]: {"kind": "wall"}, z["ymin"]: {"kind": "wall"}, z["ymax"]: {"kind": "wall"},
+           z["zmin"]: {"kind": "symmetry"}, z["zmax"]: {"kind": "symmetry"}}
+    b = Boundary(m, bcs, 1.0)
+    o = OracleSolver(m, fluid_of({"rho": 1.0, "mu": 0.1}), bcs, advection=1.0)
+    np.testing.assert_array_equal(b.sym, o.sym)
+    assert b.pin == o._pin
+    np.testing.assert_array_equal(b.p_fixed, o.p_fixed)

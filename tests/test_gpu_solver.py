@@ -93,3 +93,60 @@ def test_pipe_matches_reference(name, linear):
     np.testing.assert_allclose(f["P"], P, atol=1e-8 * np.ptp(P))
     assert abs(rep["history"][-1]["imbalance"]) < 1e-11
     s.close()
+
+
+def test_transient_bdf2_matches_reference():
+    from fixtures import transient_bcs
+    from zvcfd_b200.solver import B200Solver
+
+    g = load("transient_pipe")
+    m = mesh_of(g)
+    s = B200Solver(m, fluid_of(g), transient_bcs(g, m), advection=1.0, linear_rtol=0.1)
+    rep = s.solve(max_iterations=800, tol=1e-11)
+    assert rep["converged"]
+    np.testing.assert_allclose(s.fields()["U"], g["U0"], atol=1e-8 * np.abs(g["U0"]).max())
+    rep = s.solve_transient(float(g["dt"]), int(g["steps"]), scheme="bdf2", loops=60, tol=1e-11)
+    assert rep["converged"]
+    f = s.fields()
+    np.testing.assert_allclose(f["U"], g["U"], atol=1e-8 * np.abs(g["U"]).max())
+    np.testing.assert_allclose(f["P"], g["P"], atol=1e-8 * np.ptp(g["P"]))
+    s.close()
+
+
+def test_steady_rcr_outlet_reaches_its_0d_law():
+    """A steady RCR outlet ends at p = a + r Q with Q the outlet's flow (the property of the
+    reference's tests/test_fv_boundaries.py:88-110), and the mass balance is exact."""
+    from zvcfd_b200.lumped import RCR
+    from zvcfd_b200.solver import B200Solver
+
+    g = load("pipe_reference_tube")
+    m = mesh_of(g)
+    bcs = pipe_bcs("pipe_reference_tube", g, m)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    model = RCR(rp=0.5, c=1e-3, rd=2.0)
+    bcs[z["outlet"]] = {"kind": "pressure", "value": 0.0, "lumped": model}
+    s = B200Solver(m, fluid_of(g), bcs, advection=1.0)
+    rep = s.solve(max_iterations=800, tol=1e-11)
+    assert rep["converged"], rep["history"][-1]
+    q = s.patch_flows()
+    Q = q[z["outlet"]]
+    P = s.fields()["P"]
+    nodes = np.unique(m.zones[z["outlet"]].faces)
+    nodes = nodes[nodes >= 0]
+    a, r = model.steady_coefficients()
+    np.testing.assert_allclose(P[nodes], a + r * Q, rtol=1e-8, atol=1e-10)
+    assert abs(sum(q.values())) < 1e-11 * sum(abs(v) for v in q.values())
+    s.close()
+
+
+@pytest.mark.parametrize("name", ["pipe_reference_tube", "curved_cy"])
+def test_wall_shear_matches_reference(name):
+    from zvcfd_b200.wall import WallShear
+
+    g = load(name)
+    m = mesh_of(g)
+    fl = fluid_of(g)
+    wall = [z for z, zz in m.zones.items() if zz.name == "wall"]
+    tau = WallShear(m, wall)(g["U"], viscosity=fl.viscosity, mu=fl.mu).cpu().numpy()
+    ref = load("wall_shear")[f"{name}_tau"]
+    np.testing.assert_allclose(tau, ref, atol=1e-12 * np.abs(ref).max())

@@ -53,3 +53,32 @@ def test_oracle_reaches_reference_solution(name):
     np.testing.assert_allclose(s.P, g["P"], atol=1e-9 * np.ptp(g["P"]))
     flows = s.zone_flows()
     assert abs(sum(flows.values())) < 1e-11 * sum(abs(v) for v in flows.values())
+
+
+def test_oracle_transient_matches_reference():
+    from fixtures import fluid_of, mesh_of, transient_bcs
+    from oracle.fv import OracleSolver
+
+    g = load("transient_pipe")
+    m = mesh_of(g)
+    s = OracleSolver(m, fluid_of(g), transient_bcs(g, m), advection=1.0)
+    rep = s.solve(max_iterations=400, tol=1e-12)
+    assert rep["converged"]
+    np.testing.assert_allclose(s.U, g["U0"], atol=1e-9 * np.abs(g["U0"]).max())
+    s.solve_transient(float(g["dt"]), int(g["steps"]), scheme="bdf2", loops=30, tol=1e-12)
+    np.testing.assert_allclose(s.U, g["U"], atol=1e-9 * np.abs(g["U"]).max())
+    np.testing.assert_allclose(s.P, g["P"], atol=1e-9 * np.ptp(g["P"]))
+
+
+@pytest.mark.parametrize("name", ["pipe_reference_tube", "curved_cy"])
+def test_oracle_wall_shear_matches_reference(name):
+    from fixtures import fluid_of, mesh_of
+    from oracle.wall import wall_shear
+
+    g = load(name)
+    m = mesh_of(g)
+    fl = fluid_of(g)
+    wall = [z for z, zz in m.zones.items() if zz.name == "wall"]
+    tau = wall_shear(m, wall, g["U"], mu=fl.mu, viscosity=fl.viscosity)
+    ref = load("wall_shear")[f"{name}_tau"]
+    np.testing.assert_allclose(tau, ref, atol=1e-12 * np.abs(ref).max())

@@ -32,7 +32,8 @@
 namespace zvfv {
 namespace amg {
 
-constexpr int DENSE_MAX = 32;            // block rows of a dense coarsest level (128 x 128)
+constexpr int DENSE_MAX = 24;            // block rows of a dense coarsest level (96 x 96:
+                                         // matrix and inverse fit one CTA's shared memory)
 
 // ------------------------------------------------------------------ small kernels
 

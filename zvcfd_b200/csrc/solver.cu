@@ -235,6 +235,7 @@ class Hierarchy {
         const bool rebuild = !same || prm.rebuild_every <= 1 || setups % prm.rebuild_every == 0;
         ++setups;
         values.release();
+        rebuilt_ = rebuild;
         if (rebuild) {
             structure.release();
             L.clear();
@@ -260,6 +261,19 @@ class Hierarchy {
     int vcycle(const T *b0, T *x0);   // defined below
 
    private:
+    bool rebuilt_ = false;
+
+    // level l's blocks: the sums of level l-1's blocks over each aggregate pair
+    int galerkin_values(size_t l) {
+        Level &v = L[l];
+        const Level &f = L[l - 1];
+        double *d;
+        ZV_TRY(values.get(&d, v.nnz * 16));
+        k_seg_sum<<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz, 16, f.gseg, f.gperm, f.data, d); count_launch();
+        v.data = d;
+        return launch_status("galerkin");
+    }
+
     // ---------------------------------------------------------------- sorting helpers
 
     // keys (m) -> stable order perm, unique keys, segment starts (nseg + 1)
@@ -461,6 +475,7 @@ class Hierarchy {
             c.indptr = cptr;
             c.indices = cidx;
             L.push_back(c);
+            ZV_TRY(galerkin_values(L.size() - 1));     // the next level aggregates on these
         }
         return launch_status("hierarchy structure");
     }
@@ -471,13 +486,7 @@ class Hierarchy {
     int build_values() {
         for (size_t l = 0; l < L.size(); ++l) {
             Level &v = L[l];
-            if (l > 0) {
-                const Level &f = L[l - 1];
-                double *d;
-                ZV_TRY(values.get(&d, v.nnz * 16));
-                k_seg_sum<<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz, 16, f.gseg, f.gperm, f.data, d); count_launch();
-                v.data = d;
-            }
+            if (l > 0 && !rebuilt_) ZV_TRY(galerkin_values(l));
             ZV_TRY(values.get(&v.dinv64, v.n * 16));
             k_dinv<double><<<grid_for(v.n, 128), 128, 0, st>>>(v.n, v.data, v.dpos, v.dinv64); count_launch();
             if (prm.precision == 1) {
