@@ -182,15 +182,26 @@ int zvfv_bsr_residual(int64_t n, const int64_t *indptr, const int32_t *indices,
 int zvfv_bsr_spmv_f32(int64_t n, const int64_t *indptr, const int32_t *indices,
                       const float *data, const float *x, float *y, int lanes, void *stream);
 
+/* The structure of A^T (built once per pattern): tptr int64 (n+1), per entry the row trow
+ * int32 (ascending within a column) and the block index tperm int64 of A. Replaces the
+ * reference's host transposes (BlockMatrix.to_scipy().T, zvcfd/fv/linear.py:115-135). */
+int zvfv_bsr_transpose(int64_t n, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                       int64_t *tptr, int32_t *trow, int64_t *tperm, void *stream);
+/* y = A^T x (the discrete adjoint's product; lanes 8, 16 or 32) */
+int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const int64_t *tperm,
+                    const double *data, const double *x, double *y, int lanes, void *stream);
+
 /* ---------------------------------------------------------------- linear back end */
 
 /* FGMRES preconditioned by one V-cycle of a device-built aggregation AMG: replaces the AmgX C
  * API the reference binds (AMGX_config_create / resources / matrix / solver handles,
  * zvcfd/fv/linear.py:728-739, :846-868, :905-955) and its own ACM (linear.py:328-518).
- * create: precision 0 FP64, 1 FP32 hierarchy; strength 0 block norm, 1 pressure entry. */
-int zvfv_solver_create(void **handle, int precision, int strength, int passes, int presweeps,
-                       int postsweeps, double omega, int coarse_sweeps, int max_levels,
-                       int rebuild_every, int restart);
+ * create: precision 0 FP64, 1 FP32 hierarchy; smoother 0 damped block Jacobi, 1 symmetric
+ * multicolour block Gauss-Seidel (AmgX's MULTICOLOR_GS of the `gs` preset, linear.py:76-79);
+ * strength 0 block norm, 1 pressure entry. */
+int zvfv_solver_create(void **handle, int precision, int smoother, int strength, int passes,
+                       int presweeps, int postsweeps, double omega, int coarse_sweeps,
+                       int max_levels, int rebuild_every, int restart);
 /* structure on the first call (or when it changes), coefficients after: AMGX_matrix_upload_all
  * / AMGX_matrix_replace_coefficients + AMGX_solver_setup (zvcfd/fv/linear.py:327-349, :310) */
 int zvfv_solver_setup(void *handle, int64_t n, int64_t nnzb, const int64_t *indptr,
@@ -203,6 +214,14 @@ int zvfv_solver_solve(void *handle, const double *b, double *x, double rtol, int
                       const int64_t *u_len, const int64_t *const *w_idx, const double *const *w_val,
                       const int64_t *w_len, int *iterations, double *residual, int *converged,
                       void *stream);
+/* the adjoint solve A^T x = b (same arguments): FGMRES on A^T preconditioned by the V-cycle of
+ * the same hierarchy on every level's transpose (A^T, D^-T, the dense inverse transposed);
+ * no reference counterpart (the reference has no adjoint); builds the transposes on first use */
+int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, int maxiter,
+                        int n_lowrank, const int64_t *const *u_idx, const double *const *u_val,
+                        const int64_t *u_len, const int64_t *const *w_idx,
+                        const double *const *w_val, const int64_t *w_len, int *iterations,
+                        double *residual, int *converged, void *stream);
 /* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:386-399) */
 int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
 /* hierarchy sizes (ACM.stats, zvcfd/fv/linear.py:513-518) */

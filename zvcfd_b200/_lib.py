@@ -52,9 +52,12 @@ _SIGNATURES = {
     "zvfv_bsr_spmv": ([I64, P, P, P, P, P, I32, P], None),
     "zvfv_bsr_residual": ([I64, P, P, P, P, P, P, I32, P], None),
     "zvfv_bsr_spmv_f32": ([I64, P, P, P, P, P, I32, P], None),
-    "zvfv_solver_create": ([P, I32, I32, I32, I32, I32, F64, I32, I32, I32, I32], None),
+    "zvfv_bsr_transpose": ([I64, I64, P, P, P, P, P, P], None),
+    "zvfv_bsr_spmv_t": ([I64, P, P, P, P, P, P, I32, P], None),
+    "zvfv_solver_create": ([P, I32, I32, I32, I32, I32, I32, F64, I32, I32, I32, I32], None),
     "zvfv_solver_setup": ([P, I64, I64, P, P, P, P], None),
     "zvfv_solver_solve": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
+    "zvfv_solver_solve_t": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_vcycle": ([P, P, P, P], None),
     "zvfv_solver_stats": ([P, I32, P, P, P], None),
     "zvfv_solver_level": ([P, I32, P, P, P, P, P], None),

@@ -396,6 +396,179 @@ k_jacobi(long long n, const long long *__restrict__ indptr, const int *__restric
     }
 }
 
+// The transposed sweep: x_out = x_in + omega D^-T (b - A^T x_in), A^T through the transpose
+// structure (tptr, trow, tperm) of the level; D^-T: lane r takes column r of the inverse.
+template <int G, bool FIRST, typename V, typename T>
+__global__ void __launch_bounds__(256)
+k_jacobi_t(long long n, const long long *__restrict__ tptr, const int *__restrict__ trow,
+           const long long *__restrict__ tperm, const V *__restrict__ data,
+           const V *__restrict__ dinv, const T *__restrict__ b, const T *__restrict__ xin,
+           T *__restrict__ xout, T omega) {
+    constexpr int S = G / 4;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = gid / G;
+    const int lane = threadIdx.x % G;
+    const int slot = lane / 4, r = lane % 4;
+    T acc = 0;
+    if (!FIRST && row < n) {
+        const long long q1 = tptr[row + 1];
+        for (long long q = tptr[row] + slot; q < q1; q += S) {
+            const int i = trow[q];
+            const V *blk = data + tperm[q] * 16;
+            const Vec4<T> xv = Vec4<T>::load(xin + (long long)i * 4);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc += (T)__ldg(blk + c * 4 + r) * xv.v[c];
+        }
+    }
+    if (!FIRST) {
+#pragma unroll
+        for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    }
+    T res = 0;
+    if (row < n) res = b[row * 4 + r] - acc;
+    const int base = (threadIdx.x % 32) / G * G;
+    T rc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rc[c] = __shfl_sync(0xffffffffu, res, base + c);
+    if (row < n && slot == 0) {
+        T upd = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) upd += (T)dinv[row * 16 + c * 4 + r] * rc[c];
+        const T x0 = FIRST ? (T)0 : xin[row * 4 + r];
+        xout[row * 4 + r] = x0 + omega * upd;
+    }
+}
+
+// ------------------------------------------------------------------ multicolour Gauss-Seidel
+
+// Node colouring of a level's graph (distance 1), Jones-Plassmann with the element colouring's
+// keys: an uncoloured node whose key is the smallest among its uncoloured neighbours takes the
+// lowest colour none of its neighbours holds. Nodes that win a round are not neighbours, so
+// the rounds are race-free and the colouring does not depend on thread order.
+__global__ void k_node_keys(long long n, unsigned long long *__restrict__ key) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    unsigned long long z = (unsigned long long)e + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    key[e] = (z & 0xFFFFFFFF00000000ull) | (unsigned long long)e;
+}
+
+__global__ void k_node_colour_round(long long n, const long long *__restrict__ indptr,
+                                    const int *__restrict__ idx,
+                                    const unsigned long long *__restrict__ key,
+                                    const int *__restrict__ col_in, int *__restrict__ col_out,
+                                    int *__restrict__ left) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int ci = col_in[i];
+    col_out[i] = ci;
+    if (ci >= 0) return;
+    const unsigned long long k = key[i];
+    unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
+    bool win = true;
+    for (long long p = indptr[i]; p < indptr[i + 1]; ++p) {
+        const int j = idx[p];
+        if (j == i) continue;
+        const int cj = col_in[j];
+        if (cj < 0) {
+            if (key[j] < k) { win = false; break; }
+        } else if (cj < 256) {
+            used[cj >> 6] |= 1ull << (cj & 63);
+        }
+    }
+    if (!win) {
+        atomicAdd(left, 1);
+        return;
+    }
+    int c = 0;
+    while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull)) ++c;
+    col_out[i] = c < 256 ? c : 255;          // > 256 colours cannot occur below 256 neighbours
+}
+
+// In-place block Gauss-Seidel over the rows of one colour (rows[0..count)): rows of a colour
+// are not coupled, so x_i <- x_i + omega D_i^-1 (b_i - (A x)_i) is a Jacobi step within the
+// colour and a Gauss-Seidel step across colours. ZERO: the first sweep from x = 0.
+template <int G, typename V, typename T>
+__global__ void __launch_bounds__(256)
+k_gs_colour(long long count, const int *__restrict__ rows, const long long *__restrict__ indptr,
+            const int *__restrict__ indices, const V *__restrict__ data, const V *__restrict__ dinv,
+            const T *__restrict__ b, T *__restrict__ x, T omega) {
+    constexpr int S = G / 4;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long k = gid / G;
+    const int lane = threadIdx.x % G;
+    const int slot = lane / 4, r = lane % 4;
+    const long long row = k < count ? rows[k] : 0;
+    T acc = 0;
+    if (k < count) {
+        const long long p1 = indptr[row + 1];
+        for (long long p = indptr[row] + slot; p < p1; p += S) {
+            const int j = __ldcs(indices + p);
+            const Vec4<V> a = Vec4<V>::load_stream(data + p * 16 + r * 4);
+            const T *xj = x + (long long)j * 4;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc += (T)a.v[c] * xj[c];
+        }
+    }
+#pragma unroll
+    for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    T res = 0;
+    if (k < count) res = b[row * 4 + r] - acc;
+    const int base = (threadIdx.x % 32) / G * G;
+    T rc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rc[c] = __shfl_sync(0xffffffffu, res, base + c);
+    if (k < count && slot == 0) {
+        const Vec4<V> d = Vec4<V>::load(dinv + row * 16 + r * 4);
+        T upd = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) upd += (T)d.v[c] * rc[c];
+        x[row * 4 + r] += omega * upd;
+    }
+}
+
+// the same sweep on A^T (columns of A through the transpose structure, D^-T)
+template <int G, typename V, typename T>
+__global__ void __launch_bounds__(256)
+k_gs_colour_t(long long count, const int *__restrict__ rows, const long long *__restrict__ tptr,
+              const int *__restrict__ trow, const long long *__restrict__ tperm,
+              const V *__restrict__ data, const V *__restrict__ dinv, const T *__restrict__ b,
+              T *__restrict__ x, T omega) {
+    constexpr int S = G / 4;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long k = gid / G;
+    const int lane = threadIdx.x % G;
+    const int slot = lane / 4, r = lane % 4;
+    const long long row = k < count ? rows[k] : 0;
+    T acc = 0;
+    if (k < count) {
+        const long long q1 = tptr[row + 1];
+        for (long long q = tptr[row] + slot; q < q1; q += S) {
+            const int i = trow[q];
+            const V *blk = data + tperm[q] * 16;
+            const T *xi = x + (long long)i * 4;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc += (T)__ldg(blk + c * 4 + r) * xi[c];
+        }
+    }
+#pragma unroll
+    for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    T res = 0;
+    if (k < count) res = b[row * 4 + r] - acc;
+    const int base = (threadIdx.x % 32) / G * G;
+    T rc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rc[c] = __shfl_sync(0xffffffffu, res, base + c);
+    if (k < count && slot == 0) {
+        T upd = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) upd += (T)dinv[row * 16 + c * 4 + r] * rc[c];
+        x[row * 4 + r] += omega * upd;
+    }
+}
+
 // coarse residual: rc[I] = sum over the aggregate's members (ascending) of r[i]
 template <typename T>
 __global__ void k_restrict(long long nc, const long long *__restrict__ mptr, const int *__restrict__ mem,
@@ -418,14 +591,15 @@ __global__ void k_prolong_add(long long n, const int *__restrict__ agg, const T 
     x[t] += e[(long long)agg[i] * 4 + (t % 4)];
 }
 
-// x = inv b for a dense coarsest level (m x m), one warp per output row
-template <typename V, typename T>
+// x = inv b (TRANS: inv^T b) for a dense coarsest level (m x m), one warp per output row
+template <typename V, typename T, bool TRANS = false>
 __global__ void k_dense_apply(int m, const V *__restrict__ inv, const T *__restrict__ b, T *__restrict__ x) {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x % 32;
     if (row >= m) return;
     T acc = 0;
-    for (int c = lane; c < m; c += 32) acc += (T)inv[(long long)row * m + c] * b[c];
+    for (int c = lane; c < m; c += 32)
+        acc += (T)inv[TRANS ? (long long)c * m + row : (long long)row * m + c] * b[c];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if (lane == 0) x[row] = acc;
@@ -440,6 +614,8 @@ struct Level {
     const double *data = nullptr;         // FP64 blocks (level 0: the caller's matrix)
     long long *dpos = nullptr;
     long long *rows = nullptr;            // row of every entry
+    long long *tptr = nullptr, *tperm = nullptr;   // the transpose's structure (adjoint)
+    int *trow = nullptr;
     double *dinv64 = nullptr;
     float *data32 = nullptr, *dinv32 = nullptr;
     int lanes = 8;
@@ -450,6 +626,9 @@ struct Level {
     int *mem = nullptr;
     long long *gperm = nullptr, *gseg = nullptr;   // Galerkin: fine blocks by coarse key
     long long cnnz = 0;
+    // multicolour Gauss-Seidel: rows sorted by colour, first row of each colour (host)
+    int *gs_rows = nullptr;
+    std::vector<long long> gs_off;
     // dense coarsest
     bool dense = false;
     double *inv64 = nullptr;
@@ -460,6 +639,7 @@ struct Level {
 
 struct Params {
     int precision = 0;       // 0 FP64 cycle, 1 FP32 cycle
+    int smoother = 1;        // 0 damped block Jacobi, 1 symmetric multicolour block Gauss-Seidel
     int strength = 0;        // 0 block norm, 1 pressure-pressure entry
     int passes = 2;
     int presweeps = 2, postsweeps = 2;

@@ -63,4 +63,12 @@ int zvfv_bsr_spmv_f32(int64_t n, const int64_t *indptr, const int32_t *indices,
                                                 x, nullptr, y, as_stream(stream));
 }
 
+// y = A^T x through the transpose structure of zvfv_bsr_transpose (the adjoint's product)
+int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const int64_t *tperm,
+                    const double *data, const double *x, double *y, int lanes, void *stream) {
+    return bsr_spmv_t_launch<false, double, double>(lanes, n, (const long long *)tptr, trow,
+                                                    (const long long *)tperm, data, x, nullptr, y,
+                                                    as_stream(stream));
+}
+
 }  // extern "C"

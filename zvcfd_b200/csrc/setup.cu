@@ -162,6 +162,36 @@ __global__ void k_gather_rows(const unsigned char *__restrict__ src, const long 
     else dst[r * width + b] = src[idx[r] * width + b];
 }
 
+__global__ void k_row_of_block(long long n, const long long *__restrict__ indptr,
+                               long long *__restrict__ row) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (long long p = indptr[i]; p < indptr[i + 1]; ++p) row[p] = i;
+}
+
+__global__ void k_transpose_fill(long long nnz, const long long *__restrict__ perm,
+                                 const long long *__restrict__ row, int *__restrict__ trow) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nnz) trow[q] = (int)row[perm[q]];
+}
+
+__global__ void k_col_starts(const int *__restrict__ sorted, long long nnz, long long n,
+                             long long *__restrict__ tptr) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > n) return;
+    long long lo = 0, hi = nnz;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (sorted[mid] < j) lo = mid + 1; else hi = mid;
+    }
+    tptr[j] = lo;
+}
+
+__global__ void k_iota64s(long long *p, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = i;
+}
+
 }  // namespace
 
 struct Pattern {
@@ -338,6 +368,36 @@ int zvfv_slot_order(const int32_t *colour, int64_t E, int32_t n_colours, int64_t
     k_colour_offsets<<<grid_for(n_colours + 1, 256), 256, 0, st>>>(sorted_c.p, E, n_colours,
                                                                    (long long *)offsets); count_launch();
     return launch_status("slot order");
+}
+
+// The structure of A^T for a block-CSR pattern: tptr int64 (n+1), and per entry q of
+// column j the row trow[q] (int32, ascending) and the block index tperm[q] (int64) of A.
+int zvfv_bsr_transpose(int64_t n, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                       int64_t *tptr, int32_t *trow, int64_t *tperm, void *stream) {
+    cudaStream_t st = as_stream(stream);
+    if (n <= 0 || nnz <= 0) {
+        set_error("bsr_transpose: empty pattern");
+        return BAD_ARGUMENT;
+    }
+    DevBuf<long long> idx, row;
+    DevBuf<int> cols;
+    ZV_TRY(idx.alloc(nnz, st));
+    ZV_TRY(row.alloc(nnz, st));
+    ZV_TRY(cols.alloc(nnz, st));
+    k_iota64s<<<grid_for(nnz, 256), 256, 0, st>>>(idx.p, nnz); count_launch();
+    k_row_of_block<<<grid_for(n, 256), 256, 0, st>>>(n, (const long long *)indptr, row.p); count_launch();
+    const int end_bit = bits_for((unsigned long long)n);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, indices, cols.p, idx.p, (long long *)tperm,
+                                    (int64_t)nnz, 0, end_bit, st);
+    DevBuf<unsigned char> tmp;
+    ZV_TRY(tmp.alloc(tb, st));
+    ZV_TRY(cuda_status(cub::DeviceRadixSort::SortPairs(tmp.p, tb, indices, cols.p, idx.p,
+                                                       (long long *)tperm, (int64_t)nnz, 0,
+                                                       end_bit, st), "sort"));
+    k_col_starts<<<grid_for(n + 1, 256), 256, 0, st>>>(cols.p, nnz, n, (long long *)tptr); count_launch();
+    k_transpose_fill<<<grid_for(nnz, 256), 256, 0, st>>>(nnz, (const long long *)tperm, row.p, trow); count_launch();
+    return launch_status("bsr transpose");
 }
 
 // dst[r] = src[idx[r]] (gather) or dst[idx[r]] = src[r] (scatter), rows of `width` bytes

@@ -15,6 +15,10 @@
 
 #include "amg.cuh"
 
+extern "C" int zvfv_bsr_transpose(int64_t n, int64_t nnz, const int64_t *indptr,
+                                  const int32_t *indices, int64_t *tptr, int32_t *trow,
+                                  int64_t *tperm, void *stream);
+
 namespace zvfv {
 
 using namespace amg;
@@ -215,6 +219,10 @@ struct LowRank {
 
 // ------------------------------------------------------------------ the hierarchy
 
+__global__ void k_iota_i32(int *p, long long n);
+__global__ void k_colour_starts(const int *__restrict__ sorted, long long n, int C,
+                                long long *__restrict__ off);
+
 class Hierarchy {
    public:
     Params prm;
@@ -257,8 +265,21 @@ class Hierarchy {
         return build_values();
     }
 
-    template <typename T>
-    int vcycle(const T *b0, T *x0);   // defined below
+    template <typename T, bool TRANS = false>
+    int vcycle();   // defined below
+
+    // the transpose structure of every level (built on first use, kept with the structure)
+    int ensure_transpose() {
+        for (Level &v : L) {
+            if (v.tptr) continue;
+            ZV_TRY(structure.get(&v.tptr, v.n + 1));
+            ZV_TRY(structure.get(&v.trow, v.nnz));
+            ZV_TRY(structure.get(&v.tperm, v.nnz));
+            ZV_TRY(zvfv_bsr_transpose(v.n, v.nnz, (const int64_t *)v.indptr, v.indices,
+                                      (int64_t *)v.tptr, v.trow, (int64_t *)v.tperm, st));
+        }
+        return OK;
+    }
 
    private:
     bool rebuilt_ = false;
@@ -419,6 +440,53 @@ class Hierarchy {
     }
     void k_iota_i32_launch(int *p, long long n);
 
+    // node colouring of level v and its rows in colour order (multicolour Gauss-Seidel)
+    int colour_level(Level &v) {
+        const long long n = v.n;
+        unsigned long long *key;
+        int *ca, *cb, *left, *sorted, *iota, *rows;
+        ZV_TRY(scratch.get(&key, n));
+        ZV_TRY(scratch.get(&ca, n));
+        ZV_TRY(scratch.get(&cb, n));
+        ZV_TRY(scratch.get(&left, 1));
+        ZV_TRY(scratch.get(&sorted, n));
+        ZV_TRY(scratch.get(&iota, n));
+        ZV_TRY(structure.get(&rows, n));
+        const unsigned g = grid_for(n, 256);
+        k_node_keys<<<g, 256, 0, st>>>(n, key); count_launch();
+        k_fill_int<<<g, 256, 0, st>>>(ca, n, -1); count_launch();
+        int host_left = 1;
+        for (int round = 0; round < 4096 && host_left; ++round) {
+            cudaMemsetAsync(left, 0, 4, st);
+            k_node_colour_round<<<g, 256, 0, st>>>(n, v.indptr, v.indices, key, ca, cb, left); count_launch();
+            std::swap(ca, cb);
+            cudaMemcpyAsync(&host_left, left, 4, cudaMemcpyDeviceToHost, st);
+            ZV_TRY(cuda_status(cudaStreamSynchronize(st), "node colouring"));
+        }
+        if (host_left) {
+            set_error("node colouring did not finish");
+            return NOT_CONVERGED;
+        }
+        k_iota_i32<<<g, 256, 0, st>>>(iota, n); count_launch();
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, ca, sorted, iota, rows, (int64_t)n, 0, 9, st);
+        unsigned char *tmp;
+        ZV_TRY(scratch.get(&tmp, tb));
+        ZV_TRY(cuda_status(cub::DeviceRadixSort::SortPairs(tmp, tb, ca, sorted, iota, rows, (int64_t)n,
+                                                           0, 9, st), "sort"));
+        int cmax = 0;
+        cudaMemcpyAsync(&cmax, sorted + n - 1, 4, cudaMemcpyDeviceToHost, st);
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colours"));
+        long long *off;
+        ZV_TRY(scratch.get(&off, cmax + 2));
+        k_colour_starts<<<grid_for(cmax + 2, 256), 256, 0, st>>>(sorted, n, cmax + 1, off); count_launch();
+        v.gs_off.assign(cmax + 2, 0);
+        cudaMemcpyAsync(v.gs_off.data(), off, (cmax + 2) * sizeof(long long), cudaMemcpyDeviceToHost, st);
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colour offsets"));
+        v.gs_rows = rows;
+        return launch_status("node colouring");
+    }
+
     int build_structure() {
         for (size_t l = 0;; ++l) {
             Level &v = L[l];
@@ -428,6 +496,10 @@ class Hierarchy {
             k_diag_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.indices, nullptr, nullptr,
                                                           v.dpos); count_launch();
             k_rows_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.rows); count_launch();
+            if (prm.smoother == 1 && v.n > DENSE_MAX) {
+                ZV_TRY(colour_level(v));
+                scratch.release();
+            }
             if (v.n <= DENSE_MAX) {
                 v.dense = true;
                 break;
@@ -530,9 +602,21 @@ class Hierarchy {
         return launch_status("hierarchy values");
     }
 
-    template <typename T>
+    template <typename T, bool TRANS>
     int cycle(size_t l);
 };
+
+__global__ void k_colour_starts(const int *__restrict__ sorted, long long n, int C,
+                                long long *__restrict__ off) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > C) return;
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (sorted[mid] < c) lo = mid + 1; else hi = mid;
+    }
+    off[c] = lo;
+}
 
 __global__ void k_iota_i32(int *p, long long n) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -577,6 +661,49 @@ void jacobi(int lanes, long long n, const long long *indptr, const int *indices,
     }
 }
 
+template <bool FIRST, typename V, typename T>
+void jacobi_t(int lanes, long long n, const Level &v, const V *data, const V *dinv, const T *b,
+              const T *xin, T *xout, T omega, cudaStream_t st) {
+    switch (lanes) {
+        case 8:
+            k_jacobi_t<8, FIRST, V, T><<<grid_for(n * 8, 256), 256, 0, st>>>(n, v.tptr, v.trow, v.tperm, data,
+                                                                           dinv, b, xin, xout, omega); count_launch();
+            break;
+        case 16:
+            k_jacobi_t<16, FIRST, V, T><<<grid_for(n * 16, 256), 256, 0, st>>>(n, v.tptr, v.trow, v.tperm, data,
+                                                                             dinv, b, xin, xout, omega); count_launch();
+            break;
+        default:
+            k_jacobi_t<32, FIRST, V, T><<<grid_for(n * 32, 256), 256, 0, st>>>(n, v.tptr, v.trow, v.tperm, data,
+                                                                             dinv, b, xin, xout, omega); count_launch();
+    }
+}
+
+// one Gauss-Seidel pass over the colours of level v, forward or backward (TRANS: on A^T)
+template <bool TRANS, typename V, typename T>
+void gs_pass(const Level &v, const V *data, const V *dinv, const T *b, T *x, T omega, bool backward,
+             cudaStream_t st) {
+    const int C = (int)v.gs_off.size() - 1;
+    for (int q = 0; q < C; ++q) {
+        const int c = backward ? C - 1 - q : q;
+        const long long o = v.gs_off[c], cnt = v.gs_off[c + 1] - v.gs_off[c];
+        if (cnt <= 0) continue;
+        const int *rows = v.gs_rows + o;
+        const int G = v.lanes;
+        const unsigned grid = grid_for(cnt * G, 256);
+        if (TRANS) {
+            if (G == 8) k_gs_colour_t<8, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
+            else if (G == 16) k_gs_colour_t<16, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
+            else k_gs_colour_t<32, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
+        } else {
+            if (G == 8) k_gs_colour<8, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.indptr, v.indices, data, dinv, b, x, omega);
+            else if (G == 16) k_gs_colour<16, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.indptr, v.indices, data, dinv, b, x, omega);
+            else k_gs_colour<32, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.indptr, v.indices, data, dinv, b, x, omega);
+        }
+        count_launch();
+    }
+}
+
 template <typename T>
 struct CyclePick;
 template <>
@@ -592,41 +719,76 @@ struct CyclePick<float> {
     static const float *inv(const Level &v) { return v.inv32; }
 };
 
-// one V-cycle on level l: L[l].b -> L[l].x (zero initial guess)
-template <typename T>
+// one V-cycle on level l: L[l].b -> L[l].x (zero initial guess); TRANS: the same cycle on
+// every level's transpose (A^T, D^-T, inv^T), reusing the hierarchy built for A
+template <typename T, bool TRANS>
 int Hierarchy::cycle(size_t l) {
     Level &v = L[l];
     T *b = static_cast<T *>(v.b);
     if (v.dense) {
         const int m = (int)(4 * v.n);
-        k_dense_apply<T, T><<<grid_for((long long)m * 32, 256), 256, 0, st>>>(
+        k_dense_apply<T, T, TRANS><<<grid_for((long long)m * 32, 256), 256, 0, st>>>(
             m, CyclePick<T>::inv(v), b, static_cast<T *>(v.x)); count_launch();
         return OK;
     }
     const auto *data = CyclePick<T>::data(v);
     const auto *dinv = CyclePick<T>::dinv(v);
+    using V = typename std::remove_const<typename std::remove_pointer<decltype(data)>::type>::type;
     const T omega = (T)prm.omega;
     const bool last = (l + 1 == L.size()) || v.agg == nullptr;
     const int pre = last ? prm.coarse_sweeps : prm.presweeps;
-    jacobi<true>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, (const T *)nullptr,
-                 static_cast<T *>(v.x), omega, st);
+    if (prm.smoother == 1 && !v.gs_off.empty()) {
+        T *x = static_cast<T *>(v.x);
+        auto sgs = [&](int sweeps) {      // symmetric: forward then backward over the colours
+            for (int s = 0; s < sweeps; ++s) {
+                gs_pass<TRANS, V, T>(v, data, dinv, b, x, omega, false, st);
+                gs_pass<TRANS, V, T>(v, data, dinv, b, x, omega, true, st);
+            }
+        };
+        cudaMemsetAsync(x, 0, v.n * 4 * sizeof(T), st);
+        sgs(pre);
+        if (last) return launch_status("coarse smoothing");
+        T *r = static_cast<T *>(v.r);
+        if (TRANS)
+            ZV_TRY(bsr_spmv_t_launch<true, V, T>(v.lanes, v.n, v.tptr, v.trow, v.tperm, data, x, b, r, st));
+        else
+            ZV_TRY(bsr_spmv_launch<true, V, T>(v.lanes, v.n, v.indptr, v.indices, data, x, b, r, st));
+        Level &c = L[l + 1];
+        k_restrict<T><<<grid_for(c.n * 4, 256), 256, 0, st>>>(c.n, v.mptr, v.mem, r, static_cast<T *>(c.b)); count_launch();
+        ZV_TRY((cycle<T, TRANS>(l + 1)));
+        k_prolong_add<T><<<grid_for(v.n * 4, 256), 256, 0, st>>>(v.n, v.agg, static_cast<const T *>(c.x), x); count_launch();
+        sgs(prm.postsweeps);
+        return launch_status("v-cycle");
+    }
+    auto sweep = [&](bool first, const T *xin, T *xout) {
+        if (TRANS) {
+            if (first) jacobi_t<true>(v.lanes, v.n, v, data, dinv, b, xin, xout, omega, st);
+            else jacobi_t<false>(v.lanes, v.n, v, data, dinv, b, xin, xout, omega, st);
+        } else {
+            if (first) jacobi<true>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, xin, xout, omega, st);
+            else jacobi<false>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, xin, xout, omega, st);
+        }
+    };
+    sweep(true, nullptr, static_cast<T *>(v.x));
     for (int s = 1; s < pre; ++s) {
-        jacobi<false>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, static_cast<const T *>(v.x),
-                      static_cast<T *>(v.x2), omega, st);
+        sweep(false, static_cast<const T *>(v.x), static_cast<T *>(v.x2));
         std::swap(v.x, v.x2);
     }
     if (last) return launch_status("coarse smoothing");
     T *r = static_cast<T *>(v.r);
-    ZV_TRY(bsr_spmv_launch<true, typename std::remove_const<typename std::remove_pointer<decltype(data)>::type>::type, T>(
-        v.lanes, v.n, v.indptr, v.indices, data, static_cast<const T *>(v.x), b, r, st));
+    if (TRANS)
+        ZV_TRY(bsr_spmv_t_launch<true, V, T>(v.lanes, v.n, v.tptr, v.trow, v.tperm, data,
+                                             static_cast<const T *>(v.x), b, r, st));
+    else
+        ZV_TRY(bsr_spmv_launch<true, V, T>(v.lanes, v.n, v.indptr, v.indices, data,
+                                           static_cast<const T *>(v.x), b, r, st));
     Level &c = L[l + 1];
     k_restrict<T><<<grid_for(c.n * 4, 256), 256, 0, st>>>(c.n, v.mptr, v.mem, r, static_cast<T *>(c.b)); count_launch();
-    ZV_TRY(cycle<T>(l + 1));
+    ZV_TRY((cycle<T, TRANS>(l + 1)));
     k_prolong_add<T><<<grid_for(v.n * 4, 256), 256, 0, st>>>(v.n, v.agg, static_cast<const T *>(c.x),
                                                             static_cast<T *>(v.x)); count_launch();
     for (int s = 0; s < prm.postsweeps; ++s) {
-        jacobi<false>(v.lanes, v.n, v.indptr, v.indices, data, dinv, b, static_cast<const T *>(v.x),
-                      static_cast<T *>(v.x2), omega, st);
+        sweep(false, static_cast<const T *>(v.x), static_cast<T *>(v.x2));
         std::swap(v.x, v.x2);
     }
     return launch_status("v-cycle");
@@ -683,13 +845,25 @@ struct Solver {
         return OK;
     }
 
-    // y = A x (+ rank-one terms); resid: y = b - A x
-    int apply(const double *xin, const double *b, double *out, const std::vector<LowRank> &lr) {
-        if (b) ZV_TRY(bsr_spmv_launch<true, double, double>(lanes0, n, indptr, indices, data, xin, b, out, st));
-        else ZV_TRY(bsr_spmv_launch<false, double, double>(lanes0, n, indptr, indices, data, xin, nullptr, out, st));
+    // y = A x (+ rank-one terms); resid: y = b - A x. trans: A^T, the rank-one terms w u^T.
+    int apply(const double *xin, const double *b, double *out, const std::vector<LowRank> &lr,
+              bool trans = false) {
+        if (trans) {
+            const Level &v0 = H.L[0];
+            if (b) ZV_TRY(bsr_spmv_t_launch<true, double, double>(lanes0, n, v0.tptr, v0.trow, v0.tperm, data, xin, b, out, st));
+            else ZV_TRY(bsr_spmv_t_launch<false, double, double>(lanes0, n, v0.tptr, v0.trow, v0.tperm, data, xin, nullptr, out, st));
+        } else {
+            if (b) ZV_TRY(bsr_spmv_launch<true, double, double>(lanes0, n, indptr, indices, data, xin, b, out, st));
+            else ZV_TRY(bsr_spmv_launch<false, double, double>(lanes0, n, indptr, indices, data, xin, nullptr, out, st));
+        }
         for (const LowRank &t : lr) {
-            k_lr_dot<<<1, 256, 0, st>>>(t.nw, t.wi, t.wv, xin, lr_t); count_launch();
-            k_lr_axpy<<<grid_for(t.nu, 256), 256, 0, st>>>(t.nu, t.ui, t.uv, lr_t, b ? -1.0 : 1.0, out); count_launch();
+            if (trans) {
+                k_lr_dot<<<1, 256, 0, st>>>(t.nu, t.ui, t.uv, xin, lr_t); count_launch();
+                k_lr_axpy<<<grid_for(t.nw, 256), 256, 0, st>>>(t.nw, t.wi, t.wv, lr_t, b ? -1.0 : 1.0, out); count_launch();
+            } else {
+                k_lr_dot<<<1, 256, 0, st>>>(t.nw, t.wi, t.wv, xin, lr_t); count_launch();
+                k_lr_axpy<<<grid_for(t.nu, 256), 256, 0, st>>>(t.nu, t.ui, t.uv, lr_t, b ? -1.0 : 1.0, out); count_launch();
+            }
         }
         return launch_status("operator");
     }
@@ -700,27 +874,27 @@ struct Solver {
         return launch_status("dot");
     }
 
-    int precondition(const double *in, double *out) {
+    int precondition(const double *in, double *out, bool trans = false) {
+        Level &v0 = H.L[0];
         if (H.prm.precision == 1) {
-            Level &v0 = H.L[0];
             k_convert<double, float><<<grid_for(n4, 256), 256, 0, st>>>(n4, in, static_cast<float *>(v0.b)); count_launch();
-            ZV_TRY(H.vcycle<float>(nullptr, nullptr));
+            ZV_TRY(trans ? H.vcycle<float, true>() : H.vcycle<float, false>());
             k_convert<float, double><<<grid_for(n4, 256), 256, 0, st>>>(n4, static_cast<const float *>(v0.x), out); count_launch();
         } else {
-            Level &v0 = H.L[0];
             cudaMemcpyAsync(v0.b, in, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
-            ZV_TRY(H.vcycle<double>(nullptr, nullptr));
+            ZV_TRY(trans ? H.vcycle<double, true>() : H.vcycle<double, false>());
             cudaMemcpyAsync(out, v0.x, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
         }
         return launch_status("precondition");
     }
 
     int solve(const double *b, double *xio, double rtol, int maxiter, const std::vector<LowRank> &lr,
-              int *iterations, double *residual, int *converged) {
+              int *iterations, double *residual, int *converged, bool trans = false) {
         const int m = restart;
+        if (trans) ZV_TRY(H.ensure_transpose());
         const int ldh = m + 1;
         cudaMemcpyAsync(x, xio, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
-        ZV_TRY(apply(x, b, r, lr));
+        ZV_TRY(apply(x, b, r, lr, trans));
         ZV_TRY(dot2(b, b, nrm));
         ZV_TRY(dot2(r, r, nrm + 1));
         cudaMemcpyAsync(host, nrm, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -738,8 +912,8 @@ struct Solver {
             int kk = 0;
             for (int k = 0; k < m; ++k) {
                 double *vk = V + (size_t)k * n4, *zk = Z + (size_t)k * n4;
-                ZV_TRY(precondition(vk, zk));
-                ZV_TRY(apply(zk, nullptr, w, lr));
+                ZV_TRY(precondition(vk, zk, trans));
+                ZV_TRY(apply(zk, nullptr, w, lr, trans));
                 const int nv = k + 1;
                 k_arnoldi_pass<0><<<ncta, DOT_THREADS, 0, st>>>(n4, V, n4, nv, nullptr, w, partial); count_launch();
                 k_fold_cols<<<1, MAXV, 0, st>>>(ncta, nv, partial, h1); count_launch();
@@ -760,7 +934,7 @@ struct Solver {
             }
             k_upper_solve<<<1, 1, 0, st>>>(kk, ldh, Hm, g, y); count_launch();
             k_combine<<<ncta, 256, 0, st>>>(n4, Z, n4, kk, y, x); count_launch();
-            ZV_TRY(apply(x, b, r, lr));
+            ZV_TRY(apply(x, b, r, lr, trans));
             ZV_TRY(dot2(r, r, nrm));
             cudaMemcpyAsync(host, nrm, sizeof(double), cudaMemcpyDeviceToHost, st);
             ZV_TRY(cuda_status(cudaStreamSynchronize(st), "restart"));
@@ -779,9 +953,9 @@ struct Solver {
 
 }  // namespace
 
-template <typename T>
-int Hierarchy::vcycle(const T *, T *) {
-    return cycle<T>(0);
+template <typename T, bool TRANS>
+int Hierarchy::vcycle() {
+    return cycle<T, TRANS>(0);
 }
 
 }  // namespace zvfv
@@ -790,16 +964,17 @@ using namespace zvfv;
 
 extern "C" {
 
-int zvfv_solver_create(void **handle, int precision, int strength, int passes, int presweeps,
-                       int postsweeps, double omega, int coarse_sweeps, int max_levels,
-                       int rebuild_every, int restart) {
-    if (!handle || precision < 0 || precision > 1 || restart < 1 || restart > MAXV - 1 || passes < 1 ||
-        presweeps < 1 || postsweeps < 0 || max_levels < 1) {
+int zvfv_solver_create(void **handle, int precision, int smoother, int strength, int passes,
+                       int presweeps, int postsweeps, double omega, int coarse_sweeps,
+                       int max_levels, int rebuild_every, int restart) {
+    if (!handle || precision < 0 || precision > 1 || smoother < 0 || smoother > 1 || restart < 1 ||
+        restart > MAXV - 1 || passes < 1 || presweeps < 1 || postsweeps < 0 || max_levels < 1) {
         set_error("solver_create: bad arguments");
         return BAD_ARGUMENT;
     }
     Solver *s = new Solver;
     s->H.prm.precision = precision;
+    s->H.prm.smoother = smoother;
     s->H.prm.strength = strength;
     s->H.prm.passes = passes;
     s->H.prm.presweeps = presweeps;
@@ -842,11 +1017,32 @@ int zvfv_solver_solve(void *handle, const double *b, double *x, double rtol, int
         return BAD_ARGUMENT;
     }
     s->st = as_stream(stream);
+    s->H.st = s->st;
     std::vector<LowRank> lr;
     for (int q = 0; q < n_lowrank; ++q)
         lr.push_back({(const long long *)u_idx[q], u_val[q], (long long)u_len[q],
                       (const long long *)w_idx[q], w_val[q], (long long)w_len[q]});
     return s->solve(b, x, rtol, maxiter, lr, iterations, residual, converged);
+}
+
+// the adjoint solve: A^T x = b with the same hierarchy, transposed (same arguments)
+int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, int maxiter,
+                        int n_lowrank, const int64_t *const *u_idx, const double *const *u_val,
+                        const int64_t *u_len, const int64_t *const *w_idx,
+                        const double *const *w_val, const int64_t *w_len, int *iterations,
+                        double *residual, int *converged, void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || !s->data || !b || !x || maxiter < 0) {
+        set_error("solver_solve_t: not set up or bad arguments");
+        return BAD_ARGUMENT;
+    }
+    s->st = as_stream(stream);
+    s->H.st = s->st;
+    std::vector<LowRank> lr;
+    for (int q = 0; q < n_lowrank; ++q)
+        lr.push_back({(const long long *)u_idx[q], u_val[q], (long long)u_len[q],
+                      (const long long *)w_idx[q], w_val[q], (long long)w_len[q]});
+    return s->solve(b, x, rtol, maxiter, lr, iterations, residual, converged, true);
 }
 
 int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream) {
@@ -856,6 +1052,7 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream) {
         return BAD_ARGUMENT;
     }
     s->st = as_stream(stream);
+    s->H.st = s->st;
     return s->precondition(r, z);
 }
 

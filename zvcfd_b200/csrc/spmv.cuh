@@ -116,4 +116,56 @@ inline int bsr_spmv_launch(int lanes, long long n, const long long *indptr, cons
     return launch_status("bsr_spmv");
 }
 
+// y = A^T x (RESID: b - A^T x) through the transpose's structure: for block row j of A^T,
+// tptr[j]..tptr[j+1] list the blocks p = tperm[q] of column j of A with their rows trow[q]
+// (rows ascending). Lane r of a slot forms column r of the block: the four lanes of a slot
+// still read the block's 128 contiguous bytes, in four 32-byte rounds.
+template <int G, bool RESID, typename V, typename XT>
+__global__ void __launch_bounds__(256)
+k_bsr_spmv_t(long long n, const long long *__restrict__ tptr, const int *__restrict__ trow,
+             const long long *__restrict__ tperm, const V *__restrict__ data,
+             const XT *__restrict__ x, const XT *__restrict__ bvec, XT *__restrict__ y) {
+    constexpr int S = G / 4;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = gid / G;
+    const int lane = threadIdx.x % G;
+    const int slot = lane / 4, r = lane % 4;
+    XT acc = 0;
+    if (row < n) {
+        const long long q1 = tptr[row + 1];
+        for (long long q = tptr[row] + slot; q < q1; q += S) {
+            const int i = trow[q];
+            const V *blk = data + tperm[q] * 16;
+            const Vec4<XT> xv = Vec4<XT>::load(x + (long long)i * 4);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc += (XT)__ldg(blk + c * 4 + r) * xv.v[c];
+        }
+    }
+#pragma unroll
+    for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    if (row < n && slot == 0) y[row * 4 + r] = RESID ? bvec[row * 4 + r] - acc : acc;
+}
+
+template <bool RESID, typename V, typename XT>
+inline int bsr_spmv_t_launch(int lanes, long long n, const long long *tptr, const int *trow,
+                             const long long *tperm, const V *data, const XT *x, const XT *b,
+                             XT *y, cudaStream_t st) {
+    if (n <= 0) return OK;
+    switch (lanes) {
+        case 8:
+            k_bsr_spmv_t<8, RESID, V, XT><<<grid_for(n * 8, 256), 256, 0, st>>>(n, tptr, trow, tperm, data, x, b, y); count_launch();
+            break;
+        case 16:
+            k_bsr_spmv_t<16, RESID, V, XT><<<grid_for(n * 16, 256), 256, 0, st>>>(n, tptr, trow, tperm, data, x, b, y); count_launch();
+            break;
+        case 32:
+            k_bsr_spmv_t<32, RESID, V, XT><<<grid_for(n * 32, 256), 256, 0, st>>>(n, tptr, trow, tperm, data, x, b, y); count_launch();
+            break;
+        default:
+            set_error("bsr_spmv_t: lanes per row %d (8, 16 or 32)", lanes);
+            return BAD_ARGUMENT;
+    }
+    return launch_status("bsr_spmv_t");
+}
+
 }  // namespace zvfv

@@ -350,3 +350,66 @@ def curved_tube(radius: float = 2e-3, bend: float = 20e-3, angle: float = np.pi 
 
 __all__ = ["Mesh", "Zone", "box", "curved_tube", "jitter", "ogrid_section", "orient", "pipe",
            "split_hexes", "split_wedges"]
+
+
+def y_bifurcation(h: float = 0.25e-3, *, parent=(2e-3, 30e-3), daughters=((1.6e-3, 25e-3, 35.0),
+                                                                      (1.4e-3, 25e-3, -35.0)),
+                  jitter_amount: float = 0.0, seed: int = 0) -> Mesh:
+    """A Y-bifurcation of seeded tetrahedra on a voxel lattice of spacing ``h``.
+
+    The parent tube (radius, length) runs along +z and ends at the origin; each daughter
+    (radius, length, angle in degrees in the x-z plane) starts there. Lattice cells whose
+    centres lie inside a tube or the junction sphere are kept and cut into six tetrahedra
+    each (conforming). The walls are stair-stepped at the lattice scale: a synthetic mesh
+    with the sizes and coupling of a vessel, not a body-fitted one. Zones: 3 ``inlet``
+    (the parent's end plane), 4 ``outlet1``, 5 ``outlet2`` (the daughters' end caps),
+    6 ``wall``.
+    """
+    Rp, Lp = parent
+    axes = [(np.array([0.0, 0.0, -Lp]), np.array([0.0, 0.0, 1.0]), Lp, Rp)]
+    for R, L, ang in daughters:
+        a = np.radians(ang)
+        axes.append((np.zeros(3), np.array([np.sin(a), 0.0, np.cos(a)]), L, R))
+    ends = [o + d * L for o, d, L, _ in axes[1:]]
+    lo = np.minimum.reduce([np.array([-Rp, -Rp, -Lp])] + [e - max(R for *_, R in axes) for e in ends])
+    hi = np.maximum.reduce([np.array([Rp, Rp, 0.0])] + [e + max(R for *_, R in axes) for e in ends])
+    n = np.ceil((hi - lo) / h).astype(int)
+    lo[2] = -Lp                                   # the inlet is a lattice plane
+    n[2] = int(np.ceil((hi[2] - lo[2]) / h))
+
+    def inside(p):
+        ok = np.linalg.norm(p, axis=1) < Rp
+        for o, d, L, R in axes:
+            t = (p - o) @ d
+            r = np.linalg.norm((p - o) - t[:, None] * d, axis=1)
+            ok |= (t >= 0) & (t <= L) & (r < R)
+        return ok
+
+    ii, jj, kk = np.meshgrid(np.arange(n[0]), np.arange(n[1]), np.arange(n[2]), indexing="ij")
+    cells = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], 1)
+    keep = cells[inside(lo + (cells + 0.5) * h)]
+    # corner node ids on the (n+1)^3 lattice, renumbered densely in z-major order
+    corners = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                        [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+    lat = (keep[:, None, :] + corners[None]).reshape(-1, 3)
+    key = (lat[:, 2] * (n[1] + 1) + lat[:, 1]) * (n[0] + 1) + lat[:, 0]
+    ukey, inv = np.unique(key, return_inverse=True)
+    hexes = inv.reshape(-1, 8)
+    kz, rem = np.divmod(ukey, (n[1] + 1) * (n[0] + 1))
+    ky, kx = np.divmod(rem, n[0] + 1)
+    nodes = lo + np.stack([kx, ky, kz], 1) * h
+    tets = split_wedges(split_hexes(hexes))
+    mesh = Mesh(nodes, {"tet": orient(nodes, "tet", tets)})
+
+    def classify(c, nrm):
+        w = np.full(len(c), 3)
+        w[np.abs(c[:, 2] + Lp) < 1e-9 * Lp] = 0
+        for q, (o, d, L, R) in enumerate(axes[1:]):
+            t = (c - o) @ d
+            w[(w == 3) & (t > L - 0.75 * h) & (nrm @ d > 0.5)] = 1 + q
+        return w
+
+    mesh.zones = _zones(mesh, classify, [("inlet", "velocity-inlet"), ("outlet1", "pressure-outlet"),
+                                         ("outlet2", "pressure-outlet"), ("wall", "wall")])
+    jitter(mesh, jitter_amount, seed)
+    return mesh
