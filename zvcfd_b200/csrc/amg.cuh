@@ -612,6 +612,7 @@ struct Level {
     const long long *indptr = nullptr;
     const int *indices = nullptr;
     const double *data = nullptr;         // FP64 blocks (level 0: the caller's matrix)
+    double *own = nullptr;                // a coarse level's own FP64 blocks
     long long *dpos = nullptr;
     long long *rows = nullptr;            // row of every entry
     long long *tptr = nullptr, *tperm = nullptr;   // the transpose's structure (adjoint)
@@ -640,6 +641,9 @@ struct Level {
 struct Params {
     int precision = 0;       // 0 FP64 cycle, 1 FP32 cycle
     int smoother = 1;        // 0 damped block Jacobi, 1 symmetric multicolour block Gauss-Seidel
+    int gs_levels = 2;       // with Gauss-Seidel: the finest levels that use it (Jacobi below)
+    int jacobi_sweeps = 2;   // damped block-Jacobi sweeps (pre and post) below them
+    double jacobi_omega = 0.7;
     int strength = 0;        // 0 block norm, 1 pressure-pressure entry
     int passes = 2;
     int presweeps = 2, postsweeps = 2;

@@ -239,12 +239,14 @@ class Hierarchy {
         structure.set_stream(s);
         values.set_stream(s);
         scratch.set_stream(s);
+        persist.set_stream(s);
         const bool same = L.size() && n == src_n && nnz == src_nnz && indptr == src_indptr;
         const bool rebuild = !same || prm.rebuild_every <= 1 || setups % prm.rebuild_every == 0;
         ++setups;
-        values.release();
         rebuilt_ = rebuild;
         if (rebuild) {
+            drop_graphs();
+            values.release();
             structure.release();
             L.clear();
             Level l0;
@@ -258,11 +260,28 @@ class Hierarchy {
             src_n = n;
             src_nnz = nnz;
             ZV_TRY(build_structure());
+            ZV_TRY(allocate_values());
         } else {
+            if (L[0].data != data || L[0].indices != indices) drop_graphs();
             L[0].data = data;
             L[0].indices = indices;
+            for (size_t l = 1; l < L.size(); ++l) ZV_TRY(galerkin_values(l));
         }
-        return build_values();
+        return compute_values();
+    }
+
+    ~Hierarchy() {
+        drop_graphs();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+    }
+
+    void drop_graphs() {
+        for (auto &row : graphs)
+            for (cudaGraphExec_t &g : row)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
     }
 
     template <typename T, bool TRANS = false>
@@ -281,17 +300,24 @@ class Hierarchy {
         return OK;
     }
 
+    cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [FP32][TRANS]
+    cudaStream_t capture_stream = nullptr;
+
    private:
     bool rebuilt_ = false;
+    Arena persist;                         // kept across rebuilds: the finest level's colouring
+    const long long *coloured_indptr = nullptr;
+    long long coloured_n = -1, coloured_nnz = -1;
+    int *c0_rows = nullptr;
+    std::vector<long long> c0_off;
 
     // level l's blocks: the sums of level l-1's blocks over each aggregate pair
     int galerkin_values(size_t l) {
         Level &v = L[l];
         const Level &f = L[l - 1];
-        double *d;
-        ZV_TRY(values.get(&d, v.nnz * 16));
-        k_seg_sum<<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz, 16, f.gseg, f.gperm, f.data, d); count_launch();
-        v.data = d;
+        if (!v.own) ZV_TRY(structure.get(&v.own, v.nnz * 16));
+        k_seg_sum<<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz, 16, f.gseg, f.gperm, f.data, v.own); count_launch();
+        v.data = v.own;
         return launch_status("galerkin");
     }
 
@@ -441,7 +467,7 @@ class Hierarchy {
     void k_iota_i32_launch(int *p, long long n);
 
     // node colouring of level v and its rows in colour order (multicolour Gauss-Seidel)
-    int colour_level(Level &v) {
+    int colour_level(Level &v, Arena &keep) {
         const long long n = v.n;
         unsigned long long *key;
         int *ca, *cb, *left, *sorted, *iota, *rows;
@@ -451,15 +477,17 @@ class Hierarchy {
         ZV_TRY(scratch.get(&left, 1));
         ZV_TRY(scratch.get(&sorted, n));
         ZV_TRY(scratch.get(&iota, n));
-        ZV_TRY(structure.get(&rows, n));
+        ZV_TRY(keep.get(&rows, n));
         const unsigned g = grid_for(n, 256);
         k_node_keys<<<g, 256, 0, st>>>(n, key); count_launch();
         k_fill_int<<<g, 256, 0, st>>>(ca, n, -1); count_launch();
         int host_left = 1;
-        for (int round = 0; round < 4096 && host_left; ++round) {
-            cudaMemsetAsync(left, 0, 4, st);
-            k_node_colour_round<<<g, 256, 0, st>>>(n, v.indptr, v.indices, key, ca, cb, left); count_launch();
-            std::swap(ca, cb);
+        for (int round = 0; round < 4096 && host_left; round += 4) {
+            for (int q = 0; q < 4; ++q) {       // a finished colouring is a fixed point
+                cudaMemsetAsync(left, 0, 4, st);
+                k_node_colour_round<<<g, 256, 0, st>>>(n, v.indptr, v.indices, key, ca, cb, left); count_launch();
+                std::swap(ca, cb);
+            }
             cudaMemcpyAsync(&host_left, left, 4, cudaMemcpyDeviceToHost, st);
             ZV_TRY(cuda_status(cudaStreamSynchronize(st), "node colouring"));
         }
@@ -496,9 +524,22 @@ class Hierarchy {
             k_diag_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.indices, nullptr, nullptr,
                                                           v.dpos); count_launch();
             k_rows_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.rows); count_launch();
-            if (prm.smoother == 1 && v.n > DENSE_MAX) {
-                ZV_TRY(colour_level(v));
-                scratch.release();
+            if (prm.smoother == 1 && v.n > DENSE_MAX && (int)l < prm.gs_levels) {
+                if (l == 0 && coloured_indptr == v.indptr && coloured_n == v.n &&
+                    coloured_nnz == v.nnz && c0_rows) {
+                    v.gs_rows = c0_rows;                  // the finest pattern does not change
+                    v.gs_off = c0_off;
+                } else {
+                    ZV_TRY(colour_level(v, l == 0 ? persist : structure));
+                    scratch.release();
+                    if (l == 0) {
+                        coloured_indptr = v.indptr;
+                        coloured_n = v.n;
+                        coloured_nnz = v.nnz;
+                        c0_rows = v.gs_rows;
+                        c0_off = v.gs_off;
+                    }
+                }
             }
             if (v.n <= DENSE_MAX) {
                 v.dense = true;
@@ -555,25 +596,45 @@ class Hierarchy {
     void k_agg_keys(const int *agg, long long n, unsigned long long *keys);
     void k_narrow(const long long *src, long long n, int *dst);
 
-    int build_values() {
-        for (size_t l = 0; l < L.size(); ++l) {
-            Level &v = L[l];
-            if (l > 0 && !rebuilt_) ZV_TRY(galerkin_values(l));
+    // buffers that live as long as the structure: pointers stay fixed across set-ups, so a
+    // captured V-cycle graph stays valid until the next rebuild
+    int allocate_values() {
+        const size_t vs = prm.precision == 1 ? sizeof(float) : sizeof(double);
+        for (Level &v : L) {
             ZV_TRY(values.get(&v.dinv64, v.n * 16));
-            k_dinv<double><<<grid_for(v.n, 128), 128, 0, st>>>(v.n, v.data, v.dpos, v.dinv64); count_launch();
             if (prm.precision == 1) {
                 ZV_TRY(values.get(&v.data32, v.nnz * 16));
                 ZV_TRY(values.get(&v.dinv32, v.n * 16));
+            }
+            if (v.dense) {
+                const size_t m = 4 * v.n;
+                ZV_TRY(values.get(&v.inv64, m * m));
+                if (prm.precision == 1) ZV_TRY(values.get(&v.inv32, m * m));
+            }
+            char *buf;
+            ZV_TRY(values.get(&buf, 4 * vs * v.n * 4));
+            v.x = buf;
+            v.x2 = buf + vs * v.n * 4;
+            v.b = buf + 2 * vs * v.n * 4;
+            v.r = buf + 3 * vs * v.n * 4;
+        }
+        return OK;
+    }
+
+    int compute_values() {
+        for (size_t l = 0; l < L.size(); ++l) {
+            Level &v = L[l];
+            k_dinv<double><<<grid_for(v.n, 128), 128, 0, st>>>(v.n, v.data, v.dpos, v.dinv64); count_launch();
+            if (prm.precision == 1) {
                 k_convert<double, float><<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz * 16, v.data, v.data32); count_launch();
                 k_convert<double, float><<<grid_for(v.n * 16, 256), 256, 0, st>>>(v.n * 16, v.dinv64, v.dinv32); count_launch();
             }
-            if (v.dense) {
+            if (v.inv64) {
                 const int m = (int)(4 * v.n);
                 double *dense;
                 int *ok;
                 ZV_TRY(scratch.get(&dense, (size_t)m * m));
                 ZV_TRY(scratch.get(&ok, 1));
-                ZV_TRY(values.get(&v.inv64, (size_t)m * m));
                 cudaMemsetAsync(dense, 0, sizeof(double) * m * m, st);
                 k_densify<<<grid_for(v.n, 64), 64, 0, st>>>(v.n, v.indptr, v.indices, v.data, dense); count_launch();
                 const size_t smem = sizeof(double) * 2 * m * m;
@@ -582,22 +643,14 @@ class Hierarchy {
                 int okh = 0;
                 cudaMemcpyAsync(&okh, ok, 4, cudaMemcpyDeviceToHost, st);
                 ZV_TRY(cuda_status(cudaStreamSynchronize(st), "coarse inverse"));
-                if (!okh) {
-                    v.dense = false;      // singular: smooth the coarsest level instead
-                } else if (prm.precision == 1) {
-                    ZV_TRY(values.get(&v.inv32, (size_t)m * m));
-                    k_convert<double, float><<<grid_for((long long)m * m, 256), 256, 0, st>>>((long long)m * m,
-                                                                                           v.inv64, v.inv32); count_launch();
-                }
+                const bool was = v.dense;
+                v.dense = okh != 0;              // singular: smooth the coarsest level instead
+                if (was != v.dense) drop_graphs();
+                if (v.dense && prm.precision == 1)
+                    k_convert<double, float><<<grid_for((long long)m * m, 256), 256, 0, st>>>(
+                        (long long)m * m, v.inv64, v.inv32); count_launch();
                 scratch.release();
             }
-            const size_t vs = prm.precision == 1 ? sizeof(float) : sizeof(double);
-            char *buf;
-            ZV_TRY(values.get(&buf, 4 * vs * v.n * 4));
-            v.x = buf;
-            v.x2 = buf + vs * v.n * 4;
-            v.b = buf + 2 * vs * v.n * 4;
-            v.r = buf + 3 * vs * v.n * 4;
         }
         return launch_status("hierarchy values");
     }
@@ -734,10 +787,13 @@ int Hierarchy::cycle(size_t l) {
     const auto *data = CyclePick<T>::data(v);
     const auto *dinv = CyclePick<T>::dinv(v);
     using V = typename std::remove_const<typename std::remove_pointer<decltype(data)>::type>::type;
-    const T omega = (T)prm.omega;
+    const bool gs_level = prm.smoother == 1 && !v.gs_off.empty();
+    const bool jac_below = prm.smoother == 1 && !gs_level;       // Jacobi below the GS levels
+    const T omega = (T)(jac_below ? prm.jacobi_omega : prm.omega);
     const bool last = (l + 1 == L.size()) || v.agg == nullptr;
-    const int pre = last ? prm.coarse_sweeps : prm.presweeps;
-    if (prm.smoother == 1 && !v.gs_off.empty()) {
+    const int pre = last ? prm.coarse_sweeps : (jac_below ? prm.jacobi_sweeps : prm.presweeps);
+    const int post = jac_below ? prm.jacobi_sweeps : prm.postsweeps;
+    if (gs_level) {
         T *x = static_cast<T *>(v.x);
         auto sgs = [&](int sweeps) {      // symmetric: forward then backward over the colours
             for (int s = 0; s < sweeps; ++s) {
@@ -787,7 +843,7 @@ int Hierarchy::cycle(size_t l) {
     ZV_TRY((cycle<T, TRANS>(l + 1)));
     k_prolong_add<T><<<grid_for(v.n * 4, 256), 256, 0, st>>>(v.n, v.agg, static_cast<const T *>(c.x),
                                                             static_cast<T *>(v.x)); count_launch();
-    for (int s = 0; s < prm.postsweeps; ++s) {
+    for (int s = 0; s < post; ++s) {
         sweep(false, static_cast<const T *>(v.x), static_cast<T *>(v.x2));
         std::swap(v.x, v.x2);
     }
@@ -953,9 +1009,36 @@ struct Solver {
 
 }  // namespace
 
+// one V-cycle (L[0].b -> L[0].x) as a CUDA graph: captured on first use after each rebuild
+// (on a stream of the handle's own: the caller's may be the legacy stream, which cannot be
+// captured) and replayed on the caller's stream; every buffer it touches keeps its address
+// until the next rebuild
 template <typename T, bool TRANS>
 int Hierarchy::vcycle() {
-    return cycle<T, TRANS>(0);
+    cudaGraphExec_t &g = graphs[sizeof(T) == 4 ? 1 : 0][TRANS ? 1 : 0];
+    if (!g) {
+        if (!capture_stream)
+            ZV_TRY(cuda_status(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking),
+                               "capture stream"));
+        cudaStream_t caller = st;
+        ZV_TRY(cuda_status(cudaStreamSynchronize(caller), "before capture"));
+        st = capture_stream;
+        cudaGraph_t graph = nullptr;
+        int rc = cuda_status(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
+        if (rc == OK) {
+            rc = cycle<T, TRANS>(0);
+            const int rc2 = cuda_status(cudaStreamEndCapture(st, &graph), "end capture");
+            if (rc == OK) rc = rc2;
+        }
+        st = caller;
+        if (rc == OK) rc = cuda_status(cudaGraphInstantiate(&g, graph, 0), "instantiate");
+        if (graph) cudaGraphDestroy(graph);
+        if (rc != OK) {
+            g = nullptr;
+            return rc;
+        }
+    }
+    return cuda_status(cudaGraphLaunch(g, st), "graph launch");
 }
 
 }  // namespace zvfv
