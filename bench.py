@@ -245,6 +245,8 @@ def main():
     ap.add_argument("--cpu-axial", type=int, default=3, help="axial cells of the CPU sample")
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nvtx", action="store_true",
+                    help="mark the timed steps with an NVTX range 'timed' (for ncu --nvtx-include)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -275,8 +277,12 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     l0 = lib.zvfv_launch_count()
+    if args.nvtx:
+        torch.cuda.nvtx.range_push("timed")
     with Clocks(local) as clk:
         elapsed, recs = run_steps(solver, args.steps)
+    if args.nvtx:
+        torch.cuda.nvtx.range_pop()
     launches = lib.zvfv_launch_count() - l0
     if dist:
         elapsed = max_over_ranks(elapsed, dist, "cuda")

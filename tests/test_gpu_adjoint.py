@@ -3,7 +3,7 @@
 On an assembled, scaled system of a golden pipe: the transposed SpMV equals the oracle's
 A^T x; the adjoint solve A^T lam = g equals the direct solution; and the autograd gradients
 of J = g . A^{-1} b with respect to b and to block entries of A equal central finite
-differences (relative step 1e-6) to 1e-5.
+differences (step 1e-2 max|b| in b, where J is linear; relative step 1e-6 in A) to 1e-5.
 """
 
 import numpy as np
@@ -56,7 +56,7 @@ def test_transposed_spmv_and_adjoint_solve():
 
 def test_linear_solve_gradients_match_finite_differences():
     """J = g . A^{-1} b: the device adjoint's dJ/db and dJ/dA equal the exact (direct-solve)
-    adjoint, and central finite differences of J (direct solves, relative step 1e-6) to 1e-5."""
+    adjoint, and central finite differences of J (direct solves) to 1e-5."""
     from zvcfd_b200.adjoint import linear_solve
     from zvcfd_b200.linear import B200AMG, BlockMatrix
 
@@ -84,7 +84,9 @@ def test_linear_solve_gradients_match_finite_differences():
 
     rng = np.random.default_rng(1)
     for k in rng.choice(4 * A.n, 4, replace=False):
-        h = 1e-6 * max(abs(bh[k]), 1e-3)
+        # J is linear in b: a step of 1e-2 of max|b| has no truncation error and keeps the
+        # difference well above the direct solves' rounding
+        h = 1e-2 * np.abs(bh).max()
         bp, bm = bh.copy(), bh.copy()
         bp[k] += h
         bm[k] -= h

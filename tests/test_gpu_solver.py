@@ -105,7 +105,8 @@ def test_transient_bdf2_matches_reference():
     rep = s.solve(max_iterations=800, tol=1e-11)
     assert rep["converged"]
     np.testing.assert_allclose(s.fields()["U"], g["U0"], atol=1e-8 * np.abs(g["U0"]).max())
-    rep = s.solve_transient(float(g["dt"]), int(g["steps"]), scheme="bdf2", loops=60, tol=1e-11)
+    rep = s.solve_transient(float(g["dt"]), int(g["steps"]), scheme="bdf2", loops=int(g["loops"]),
+                            tol=float(g["tol"]))
     assert rep["converged"]
     f = s.fields()
     np.testing.assert_allclose(f["U"], g["U"], atol=1e-8 * np.abs(g["U"]).max())

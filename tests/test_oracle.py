@@ -65,7 +65,8 @@ def test_oracle_transient_matches_reference():
     rep = s.solve(max_iterations=400, tol=1e-12)
     assert rep["converged"]
     np.testing.assert_allclose(s.U, g["U0"], atol=1e-9 * np.abs(g["U0"]).max())
-    s.solve_transient(float(g["dt"]), int(g["steps"]), scheme="bdf2", loops=30, tol=1e-12)
+    s.solve_transient(float(g["dt"]), int(g["steps"]), scheme="bdf2", loops=int(g["loops"]),
+                      tol=float(g["tol"]))
     np.testing.assert_allclose(s.U, g["U"], atol=1e-9 * np.abs(g["U"]).max())
     np.testing.assert_allclose(s.P, g["P"], atol=1e-9 * np.ptp(g["P"]))
 
