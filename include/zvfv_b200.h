@@ -158,6 +158,19 @@ int zvfv_update(int64_t n, const double *x, double *U, double *P, double *partia
 int zvfv_fold(int64_t nrows, int width, const double *partial, const int32_t *ops, double *out,
               void *stream);
 
+/* The state update of zvfv_update folded into stats[5] = {max |dU|, max |U|, max |dp|, min p,
+ * max p}, allocating nothing. No counterpart in the reference: it serves callers that cannot
+ * allocate device memory (a host program under a fixed memory budget, an outer loop that must
+ * not call cudaMalloc/cudaFree between steps). Its partial rows live in a 2.5 MiB array of the
+ * library that every GPU loading it holds until exit, which limits n to 1..16,777,216 nodes;
+ * larger n returns ZVFV_BAD_ARGUMENT with a message. The first call on each device looks up
+ * that array's device address (with the device current) and should come before any stream
+ * capture. Calls share the array: two calls that overlap on the GPU (different streams, no
+ * ordering between them) race and give wrong statistics. Results equal zvfv_update followed by
+ * zvfv_fold with ops {1, 1, 1, 2, 1} bit for bit. */
+int zvfv_update_noalloc(int64_t n, const double *x, double *U, double *P, double *stats,
+                        void *stream);
+
 /* Wall shear stress (N, 3) at wall nodes from the wall integration points of their sub-faces
  * (WallGradientShear.__call__, zvcfd/fv/wall.py:107-137): node_ptr int64 (N+1) groups the
  * ips by node; per ip the owning element's nodes elem int32 (M, 8, -1 padded), shape

@@ -48,6 +48,7 @@ _SIGNATURES = {
     "zvfv_update_partials": ([I64], I64),
     "zvfv_update": ([I64, P, P, P, P, P], None),
     "zvfv_fold": ([I64, I32, P, P, P, P], None),
+    "zvfv_update_noalloc": ([I64, P, P, P, P, P], None),
     "zvfv_wall_shear": ([I64, P, P, P, P, P, P, I32, F64, F64, F64, F64, F64, P, P], None),
     "zvfv_bsr_spmv": ([I64, P, P, P, P, P, I32, P], None),
     "zvfv_bsr_residual": ([I64, P, P, P, P, P, P, I32, P], None),

@@ -2,6 +2,8 @@
 // neighbour extremes for the limiter, the boundary/scaling pass that finishes every row of
 // the assembled system, the state update, and the deterministic reduction of per-CTA
 // partial statistics.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace zvfv {
@@ -307,6 +309,50 @@ __global__ void k_fold(long long nrows, int width, const double *__restrict__ pa
     }
 }
 
+// Scratch of the allocation-free update (zvfv_update_noalloc): the per-CTA partial rows of
+// k_update for up to NOALLOC_MAX_PARTIAL_ROWS CTAs of UPD_THREADS nodes, and the fold
+// operations of its five columns (max |dU|, max |U|, max |dp|, min p, max p). 2.5 MiB that
+// every GPU which loads the library holds until the process exits.
+constexpr long long NOALLOC_MAX_PARTIAL_ROWS = 1LL << 16;
+constexpr long long NOALLOC_MAX_NODES = NOALLOC_MAX_PARTIAL_ROWS * UPD_THREADS;  // 16,777,216
+static __device__ __align__(256) double g_update_scratch[NOALLOC_MAX_PARTIAL_ROWS * 5];
+static __device__ __align__(256) int g_update_fold_ops[5] = {1, 1, 1, 2, 1};
+
+// Device addresses of the two arrays, looked up once per device with that device current.
+// In host code the arrays' names stand for host-side shadows, never for device memory.
+struct NoallocScratch {
+    double *partial = nullptr;
+    int *ops = nullptr;
+};
+
+int noalloc_scratch(NoallocScratch *out) {
+    constexpr int MAX_DEVICES = 64;
+    static std::mutex lock;
+    static NoallocScratch table[MAX_DEVICES];
+    int dev = 0;
+    if (int rc = cuda_status(cudaGetDevice(&dev), "update_noalloc: cudaGetDevice")) return rc;
+    if (dev < 0 || dev >= MAX_DEVICES) {
+        set_error("update_noalloc: device %d beyond the %d devices it keeps addresses for", dev,
+                  MAX_DEVICES);
+        return BAD_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> guard(lock);
+    NoallocScratch &e = table[dev];
+    if (!e.partial) {
+        void *partial = nullptr, *ops = nullptr;
+        if (int rc = cuda_status(cudaGetSymbolAddress(&partial, g_update_scratch),
+                                 "update_noalloc: cudaGetSymbolAddress(scratch)"))
+            return rc;
+        if (int rc = cuda_status(cudaGetSymbolAddress(&ops, g_update_fold_ops),
+                                 "update_noalloc: cudaGetSymbolAddress(fold ops)"))
+            return rc;
+        e.ops = static_cast<int *>(ops);
+        e.partial = static_cast<double *>(partial);
+    }
+    *out = e;
+    return OK;
+}
+
 }  // namespace
 }  // namespace zvfv
 
@@ -368,6 +414,32 @@ int zvfv_fold(int64_t nrows, int width, const double *partial, const int32_t *op
     if (width <= 0) return OK;
     k_fold<<<1, 256, 0, as_stream(stream)>>>(nrows, width, partial, ops, out); count_launch();
     return launch_status("fold");
+}
+
+// The state update and its folded change statistics without any allocation, for callers
+// that cannot allocate device memory: a host program that runs under a fixed device-memory
+// budget handed out by another component, or a driver whose outer loop must not call
+// cudaMalloc/cudaFree between steps. It launches the same two kernels as zvfv_update followed
+// by zvfv_fold with ops {1, 1, 1, 2, 1}, with the partial rows in the file-scope array
+// g_update_scratch instead of a caller buffer, so its results are those of that pair bit for
+// bit. Every row the fold reads is written by k_update first: nothing has to start at zero.
+int zvfv_update_noalloc(int64_t n, const double *x, double *U, double *P, double *stats,
+                        void *stream) {
+    if (n <= 0 || n > NOALLOC_MAX_NODES) {
+        set_error("update_noalloc: %lld nodes; the static scratch holds partials for 1 to %lld "
+                  "nodes (use zvfv_update with a caller buffer beyond that limit)",
+                  (long long)n, (long long)NOALLOC_MAX_NODES);
+        return BAD_ARGUMENT;
+    }
+    NoallocScratch scratch;
+    if (int rc = noalloc_scratch(&scratch)) return rc;
+    const unsigned rows = grid_for(n, UPD_THREADS);
+    k_update<<<rows, UPD_THREADS, 0, as_stream(stream)>>>(n, x, U, P, scratch.partial);
+    count_launch();
+    if (int rc = launch_status("update_noalloc: update")) return rc;
+    k_fold<<<1, 256, 0, as_stream(stream)>>>(rows, 5, scratch.partial, scratch.ops, stats);
+    count_launch();
+    return launch_status("update_noalloc: fold");
 }
 
 }  // extern "C"
