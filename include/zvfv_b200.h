@@ -211,7 +211,10 @@ int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const i
  * zvcfd/fv/linear.py:728-739, :846-868, :905-955) and its own ACM (linear.py:328-518).
  * create: precision 0 FP64, 1 FP32 hierarchy; smoother 0 damped block Jacobi, 1 symmetric
  * multicolour block Gauss-Seidel (AmgX's MULTICOLOR_GS of the `gs` preset, linear.py:76-79);
- * strength 0 block norm, 1 pressure entry. */
+ * strength 0 block norm, 1 pressure entry. rebuild_every > 0 re-aggregates every that many
+ * set-ups (the reference's ACM, linear.py:337-348); 0 keeps the aggregates until a solve fails
+ * or needs more than 1.5 times (and 2 more than) the iterations of the first solve after the
+ * last rebuild (the reuse policy of its AmgX binding, linear.py:686-698, :837-841). */
 int zvfv_solver_create(void **handle, int precision, int smoother, int strength, int passes,
                        int presweeps, int postsweeps, double omega, int coarse_sweeps,
                        int max_levels, int rebuild_every, int restart);

@@ -3,7 +3,8 @@
 On an assembled, scaled system of a golden pipe: the transposed SpMV equals the oracle's
 A^T x; the adjoint solve A^T lam = g equals the direct solution; and the autograd gradients
 of J = g . A^{-1} b with respect to b and to block entries of A equal central finite
-differences (step 1e-2 max|b| in b, where J is linear; relative step 1e-6 in A) to 1e-5.
+differences (step 1e-2 max|b| in b, where J is linear; relative step 1e-4 on the most
+influential entries of A) to 1e-5.
 """
 
 import numpy as np
@@ -93,9 +94,12 @@ def test_linear_solve_gradients_match_finite_differences():
         fd = (J(D, bp) - J(D, bm)) / (2 * h)
         assert abs(fd - gb[k]) <= 1e-5 * max(abs(fd), abs(gb[k]), 1e-12), (k, fd, gb[k])
     flat = D.reshape(-1)
-    big = np.flatnonzero(np.abs(flat) > 1e-3 * np.abs(flat).max())
+    # entries whose perturbation moves J well above the direct solves' rounding: the 64 with
+    # the largest |D_q dJ/dD_q|; a relative step of 1e-4 keeps the O(h^2) error below 1e-7
+    influence = np.abs(flat * gA.reshape(-1))
+    big = np.argsort(-influence)[:64]
     for q in rng.choice(big, 4, replace=False):
-        h = 1e-6 * abs(flat[q])
+        h = 1e-4 * abs(flat[q])
         dp, dm = D.copy(), D.copy()
         dp.reshape(-1)[q] += h
         dm.reshape(-1)[q] -= h

@@ -239,6 +239,40 @@ __global__ void k_seg_sum(long long nseg, int W, const long long *__restrict__ s
     dst[t] = acc;
 }
 
+// The Galerkin sums of 4x4 blocks: dst[s] = sum of src[perm[q]] over q in [seg[s], seg[s+1]),
+// in that order (bit-equal to k_seg_sum with W = 16). Sixteen lanes own one coarse block: each
+// round the lanes fetch up to 16 of the segment's source indices at once, share them by
+// shuffle and issue all of their block loads before adding, so a segment of m blocks costs
+// ceil(m / 16) dependent round trips instead of 2 m.
+__global__ void __launch_bounds__(256)
+k_block_seg_sum(long long nseg, const long long *__restrict__ seg, const long long *__restrict__ perm,
+                const double *__restrict__ src, double *__restrict__ dst) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long s = t / 16;
+    const int c = (int)(t % 16);
+    const bool live = s < nseg;           // whole 16-lane groups share the fate of their segment
+    const long long q0 = live ? seg[s] : 0, q1 = live ? seg[s + 1] : 0;
+    // both halves of a warp run the same number of rounds, so every shuffle has all 32 lanes
+    long long rounds = (q1 - q0 + 15) / 16;
+    rounds = max(rounds, __shfl_xor_sync(0xffffffffu, rounds, 16));
+    double acc = 0.0;
+    for (long long rd = 0; rd < rounds; ++rd) {
+        const long long base = q0 + rd * 16;
+        const int m = (int)max(0LL, min(16LL, q1 - base));
+        const long long mine = c < m ? __ldcs(perm + base + c) : 0;
+        double v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const long long pk = __shfl_sync(0xffffffffu, mine, k, 16);
+            v[k] = k < m ? __ldcs(src + pk * 16 + c) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (k < m) acc += v[k];
+    }
+    if (live) dst[t] = acc;
+}
+
 // inverse of every row's 4x4 diagonal block (Gauss-Jordan, partial pivoting); a singular
 // block leaves a zero inverse (the row is then not smoothed)
 template <typename V>
@@ -441,75 +475,47 @@ k_jacobi_t(long long n, const long long *__restrict__ tptr, const int *__restric
 
 // ------------------------------------------------------------------ multicolour Gauss-Seidel
 
-// Node colouring of a level's graph (distance 1), Jones-Plassmann with the element colouring's
-// keys: an uncoloured node whose key is the smallest among its uncoloured neighbours takes the
-// lowest colour none of its neighbours holds. Nodes that win a round are not neighbours, so
-// the rounds are race-free and the colouring does not depend on thread order.
-__global__ void k_node_keys(long long n, unsigned long long *__restrict__ key) {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    unsigned long long z = (unsigned long long)e + 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    z = z ^ (z >> 31);
-    key[e] = (z & 0xFFFFFFFF00000000ull) | (unsigned long long)e;
-}
-
-__global__ void k_node_colour_round(long long n, const long long *__restrict__ indptr,
-                                    const int *__restrict__ idx,
-                                    const unsigned long long *__restrict__ key,
-                                    const int *__restrict__ col_in, int *__restrict__ col_out,
-                                    int *__restrict__ left) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int ci = col_in[i];
-    col_out[i] = ci;
-    if (ci >= 0) return;
-    const unsigned long long k = key[i];
-    unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
-    bool win = true;
-    for (long long p = indptr[i]; p < indptr[i + 1]; ++p) {
-        const int j = idx[p];
-        if (j == i) continue;
-        const int cj = col_in[j];
-        if (cj < 0) {
-            if (key[j] < k) { win = false; break; }
-        } else if (cj < 256) {
-            used[cj >> 6] |= 1ull << (cj & 63);
-        }
-    }
-    if (!win) {
-        atomicAdd(left, 1);
-        return;
-    }
-    int c = 0;
-    while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull)) ++c;
-    col_out[i] = c < 256 ? c : 255;          // > 256 colours cannot occur below 256 neighbours
-}
-
 // In-place block Gauss-Seidel over the rows of one colour (rows[0..count)): rows of a colour
 // are not coupled, so x_i <- x_i + omega D_i^-1 (b_i - (A x)_i) is a Jacobi step within the
-// colour and a Gauss-Seidel step across colours. ZERO: the first sweep from x = 0.
-template <int G, typename V, typename T>
+// colour and a Gauss-Seidel step across colours. A colour holds only a fraction of the rows,
+// so one launch is about one wave: each lane keeps GS_INFLIGHT blocks (and their column
+// indices) in flight before it uses them, instead of one dependent load after another.
+constexpr int GS_INFLIGHT = 4;
+
+// CONTIG: the colour is the contiguous row range [first, first + count) of a colour-ordered
+// copy (rows unused); otherwise its rows are rows[0..count) of the original numbering.
+template <int G, bool CONTIG, typename V, typename T>
 __global__ void __launch_bounds__(256)
-k_gs_colour(long long count, const int *__restrict__ rows, const long long *__restrict__ indptr,
-            const int *__restrict__ indices, const V *__restrict__ data, const V *__restrict__ dinv,
-            const T *__restrict__ b, T *__restrict__ x, T omega) {
+k_gs_colour(long long count, long long first, const int *__restrict__ rows,
+            const long long *__restrict__ indptr, const int *__restrict__ indices,
+            const V *__restrict__ data, const V *__restrict__ dinv, const T *__restrict__ b,
+            T *__restrict__ x, T omega) {
     constexpr int S = G / 4;
+    constexpr int U = GS_INFLIGHT;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long k = gid / G;
     const int lane = threadIdx.x % G;
     const int slot = lane / 4, r = lane % 4;
-    const long long row = k < count ? rows[k] : 0;
+    const long long row = k < count ? (CONTIG ? first + k : (long long)rows[k]) : 0;
     T acc = 0;
     if (k < count) {
         const long long p1 = indptr[row + 1];
-        for (long long p = indptr[row] + slot; p < p1; p += S) {
-            const int j = __ldcs(indices + p);
-            const Vec4<V> a = Vec4<V>::load_stream(data + p * 16 + r * 4);
-            const T *xj = x + (long long)j * 4;
+        for (long long p = indptr[row] + slot; p < p1; p += S * U) {
+            int j[U];
+            Vec4<V> a[U];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc += (T)a.v[c] * xj[c];
+            for (int u = 0; u < U; ++u) {
+                const long long q = p + u * S;
+                j[u] = q < p1 ? __ldcs(indices + q) : -1;
+                if (q < p1) a[u] = Vec4<V>::load_stream(data + q * 16 + r * 4);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (j[u] < 0) continue;
+                const T *xj = x + (long long)j[u] * 4;      // plain loads: x changes in the sweep
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc += (T)a[u].v[c] * xj[c];
+            }
         }
     }
 #pragma unroll
@@ -527,6 +533,39 @@ k_gs_colour(long long count, const int *__restrict__ rows, const long long *__re
         for (int c = 0; c < 4; ++c) upd += (T)d.v[c] * rc[c];
         x[row * 4 + r] += omega * upd;
     }
+}
+
+// colour-ordered copies: out[q] = data[src[q]] for 4x4 blocks (two doubles per thread)
+template <typename V>
+__global__ void k_gather_blocks(long long nnz, const long long *__restrict__ src,
+                                const double *__restrict__ data, V *__restrict__ out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nnz * 8) return;
+    const long long q = t / 8;
+    const int h = (int)(t % 8);
+    const double2 v = __ldcs(reinterpret_cast<const double2 *>(data + src[q] * 16) + h);
+    out[q * 16 + 2 * h] = (V)v.x;
+    out[q * 16 + 2 * h + 1] = (V)v.y;
+}
+
+// dst[k * W + e] = src[idx[k] * W + e] (GATHER) or dst[idx[k] * W + e] = src[k * W + e]
+template <bool GATHER, typename A, typename B>
+__global__ void k_permute_rows(long long n, int W, const int *__restrict__ idx,
+                               const A *__restrict__ src, B *__restrict__ dst) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * W) return;
+    const long long k = t / W;
+    const int e = (int)(t % W);
+    const long long j = idx[k];
+    if (GATHER) dst[t] = (B)src[j * W + e];
+    else dst[j * W + e] = (B)src[t];
+}
+
+// dst[k] = src[idx[k]]
+__global__ void k_gather_int(long long n, const int *__restrict__ idx, const int *__restrict__ src,
+                             int *__restrict__ dst) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] = src[idx[k]];
 }
 
 // the same sweep on A^T (columns of A through the transpose structure, D^-T)
@@ -630,6 +669,15 @@ struct Level {
     // multicolour Gauss-Seidel: rows sorted by colour, first row of each colour (host)
     int *gs_rows = nullptr;
     std::vector<long long> gs_off;
+    // the Gauss-Seidel levels' colour-ordered copy: row k is row gs_rows[k], its blocks in
+    // their original order with columns renumbered, so a colour is one contiguous row range
+    // (a sweep streams it like an SpMV) and every sum keeps its original order
+    long long *pptr = nullptr, *psrc = nullptr, *pdpos = nullptr;   // psrc: source block
+    int *pidx = nullptr, *pinv = nullptr;                           // pinv: row -> position
+    int *pagg = nullptr, *pmem = nullptr;        // aggregate of each position; members renumbered
+    double *pdata64 = nullptr, *pdinv64 = nullptr;
+    float *pdata32 = nullptr, *pdinv32 = nullptr;
+    void *pb = nullptr;                          // the level's right-hand side, colour-ordered
     // dense coarsest
     bool dense = false;
     double *inv64 = nullptr;
@@ -650,7 +698,8 @@ struct Params {
     double omega = 0.7;
     int coarse_sweeps = 8;
     int max_levels = 25;
-    int rebuild_every = 10;
+    int rebuild_every = 0;   // > 0: re-aggregate every this many set-ups; 0: adaptively
+    double rebuild_ratio = 1.5;   // adaptive: rebuild after a solve needing more iterations
 };
 
 inline int lanes_for(long long n, long long nnz) {

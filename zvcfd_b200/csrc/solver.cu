@@ -220,8 +220,6 @@ struct LowRank {
 // ------------------------------------------------------------------ the hierarchy
 
 __global__ void k_iota_i32(int *p, long long n);
-__global__ void k_colour_starts(const int *__restrict__ sorted, long long n, int C,
-                                long long *__restrict__ off);
 
 class Hierarchy {
    public:
@@ -241,10 +239,14 @@ class Hierarchy {
         scratch.set_stream(s);
         persist.set_stream(s);
         const bool same = L.size() && n == src_n && nnz == src_nnz && indptr == src_indptr;
-        const bool rebuild = !same || prm.rebuild_every <= 1 || setups % prm.rebuild_every == 0;
+        const bool periodic = prm.rebuild_every > 0 &&
+                              (prm.rebuild_every == 1 || setups % prm.rebuild_every == 0);
+        const bool rebuild = !same || periodic || rebuild_requested;
         ++setups;
         rebuilt_ = rebuild;
         if (rebuild) {
+            rebuild_requested = false;
+            base_iterations = -1;
             drop_graphs();
             values.release();
             structure.release();
@@ -288,7 +290,14 @@ class Hierarchy {
     int vcycle();   // defined below
 
     // the transpose structure of every level (built on first use, kept with the structure)
+    bool transposed_used = false;
     int ensure_transpose() {
+        if (!transposed_used) {
+            transposed_used = true;
+            if (prm.precision == 1)
+                for (Level &v : L)
+                    if (v.pptr) ZV_TRY(convert_original(v));
+        }
         for (Level &v : L) {
             if (v.tptr) continue;
             ZV_TRY(structure.get(&v.tptr, v.n + 1));
@@ -300,6 +309,22 @@ class Hierarchy {
         return OK;
     }
 
+    // Adaptive reuse (rebuild_every 0), the policy of the reference's AmgX binding
+    // (zvcfd/fv/linear.py:686-698, :837-841): later matrices keep the aggregates and only
+    // re-sum the coarse operators, until a solve fails or needs more than rebuild_ratio times
+    // the iterations of the first solve after the last rebuild (and at least 2 more).
+    bool rebuild_requested = false;
+    int base_iterations = -1;
+    void record_solve(int iterations, bool converged) {
+        if (prm.rebuild_every > 0) return;
+        if (base_iterations < 0) {
+            base_iterations = iterations;
+            return;
+        }
+        const double limit = std::max(prm.rebuild_ratio * base_iterations, base_iterations + 2.0);
+        if (!converged || iterations > limit) rebuild_requested = true;
+    }
+
     cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [FP32][TRANS]
     cudaStream_t capture_stream = nullptr;
 
@@ -308,15 +333,14 @@ class Hierarchy {
     Arena persist;                         // kept across rebuilds: the finest level's colouring
     const long long *coloured_indptr = nullptr;
     long long coloured_n = -1, coloured_nnz = -1;
-    int *c0_rows = nullptr;
-    std::vector<long long> c0_off;
+    Level c0;                              // the finest level's colouring and colour order
 
     // level l's blocks: the sums of level l-1's blocks over each aggregate pair
     int galerkin_values(size_t l) {
         Level &v = L[l];
         const Level &f = L[l - 1];
         if (!v.own) ZV_TRY(structure.get(&v.own, v.nnz * 16));
-        k_seg_sum<<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz, 16, f.gseg, f.gperm, f.data, v.own); count_launch();
+        k_block_seg_sum<<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz, f.gseg, f.gperm, f.data, v.own); count_launch();
         v.data = v.own;
         return launch_status("galerkin");
     }
@@ -466,53 +490,85 @@ class Hierarchy {
     }
     void k_iota_i32_launch(int *p, long long n);
 
-    // node colouring of level v and its rows in colour order (multicolour Gauss-Seidel)
+    // Node colouring of level v and its rows in colour order (multicolour Gauss-Seidel):
+    // greedy first-fit in row order on the host. Row i takes the lowest colour that none of
+    // its earlier neighbours holds; the level patterns are symmetric (element cliques and
+    // their Galerkin products), so no two rows of a colour are coupled either way. On the
+    // finest level of a hexahedral/prismatic tube this gives 8 large colours and 1-2 small
+    // ones, against 17 for a random-key Jones-Plassmann colouring: fewer, fuller launches per
+    // sweep. Run once per pattern on the finest level (kept in `persist`) and at each
+    // rebuild on the coarser Gauss-Seidel levels.
     int colour_level(Level &v, Arena &keep) {
-        const long long n = v.n;
-        unsigned long long *key;
-        int *ca, *cb, *left, *sorted, *iota, *rows;
-        ZV_TRY(scratch.get(&key, n));
-        ZV_TRY(scratch.get(&ca, n));
-        ZV_TRY(scratch.get(&cb, n));
-        ZV_TRY(scratch.get(&left, 1));
-        ZV_TRY(scratch.get(&sorted, n));
-        ZV_TRY(scratch.get(&iota, n));
-        ZV_TRY(keep.get(&rows, n));
-        const unsigned g = grid_for(n, 256);
-        k_node_keys<<<g, 256, 0, st>>>(n, key); count_launch();
-        k_fill_int<<<g, 256, 0, st>>>(ca, n, -1); count_launch();
-        int host_left = 1;
-        for (int round = 0; round < 4096 && host_left; round += 4) {
-            for (int q = 0; q < 4; ++q) {       // a finished colouring is a fixed point
-                cudaMemsetAsync(left, 0, 4, st);
-                k_node_colour_round<<<g, 256, 0, st>>>(n, v.indptr, v.indices, key, ca, cb, left); count_launch();
-                std::swap(ca, cb);
+        const long long n = v.n, nnz = v.nnz;
+        std::vector<long long> ip(n + 1);
+        std::vector<int> ix(nnz);
+        ZV_TRY(cuda_status(cudaMemcpyAsync(ip.data(), v.indptr, (n + 1) * sizeof(long long),
+                                           cudaMemcpyDeviceToHost, st), "colouring: indptr"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(ix.data(), v.indices, nnz * sizeof(int),
+                                           cudaMemcpyDeviceToHost, st), "colouring: indices"));
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colouring: pattern"));
+        std::vector<int> col(n);
+        std::vector<long long> seen;             // seen[c]: the last row with a neighbour of colour c
+        for (long long i = 0; i < n; ++i) {
+            for (long long p = ip[i]; p < ip[i + 1]; ++p) {
+                const int j = ix[p];
+                if (j < i) seen[col[j]] = i;
             }
-            cudaMemcpyAsync(&host_left, left, 4, cudaMemcpyDeviceToHost, st);
-            ZV_TRY(cuda_status(cudaStreamSynchronize(st), "node colouring"));
+            int c = 0;
+            while (c < (int)seen.size() && seen[c] == i) ++c;
+            if (c == (int)seen.size()) seen.push_back(-1);
+            col[i] = c;
         }
-        if (host_left) {
-            set_error("node colouring did not finish");
-            return NOT_CONVERGED;
+        const int C = (int)seen.size();
+        v.gs_off.assign(C + 1, 0);
+        for (long long i = 0; i < n; ++i) ++v.gs_off[col[i] + 1];
+        for (int c = 0; c < C; ++c) v.gs_off[c + 1] += v.gs_off[c];
+        std::vector<int> order(n);
+        std::vector<long long> at(v.gs_off.begin(), v.gs_off.end() - 1);
+        for (long long i = 0; i < n; ++i) order[at[col[i]]++] = (int)i;
+        // the colour-ordered structure: position k holds row order[k]
+        std::vector<int> inv(n), pidx(nnz);
+        std::vector<long long> pptr(n + 1), psrc(nnz), pdpos(n, -1);
+        for (long long k = 0; k < n; ++k) inv[order[k]] = (int)k;
+        pptr[0] = 0;
+        for (long long k = 0; k < n; ++k) {
+            const long long i = order[k], q0 = pptr[k];
+            for (long long p = ip[i]; p < ip[i + 1]; ++p) {
+                const long long q = q0 + (p - ip[i]);
+                pidx[q] = inv[ix[p]];
+                psrc[q] = p;
+                if (ix[p] == i) pdpos[k] = q;
+            }
+            pptr[k + 1] = q0 + (ip[i + 1] - ip[i]);
         }
-        k_iota_i32<<<g, 256, 0, st>>>(iota, n); count_launch();
-        size_t tb = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tb, ca, sorted, iota, rows, (int64_t)n, 0, 9, st);
-        unsigned char *tmp;
-        ZV_TRY(scratch.get(&tmp, tb));
-        ZV_TRY(cuda_status(cub::DeviceRadixSort::SortPairs(tmp, tb, ca, sorted, iota, rows, (int64_t)n,
-                                                           0, 9, st), "sort"));
-        int cmax = 0;
-        cudaMemcpyAsync(&cmax, sorted + n - 1, 4, cudaMemcpyDeviceToHost, st);
-        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colours"));
-        long long *off;
-        ZV_TRY(scratch.get(&off, cmax + 2));
-        k_colour_starts<<<grid_for(cmax + 2, 256), 256, 0, st>>>(sorted, n, cmax + 1, off); count_launch();
-        v.gs_off.assign(cmax + 2, 0);
-        cudaMemcpyAsync(v.gs_off.data(), off, (cmax + 2) * sizeof(long long), cudaMemcpyDeviceToHost, st);
-        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colour offsets"));
+        int *rows, *dinv_, *didx;
+        long long *dptr, *dsrc, *ddpos;
+        ZV_TRY(keep.get(&rows, n));
+        ZV_TRY(keep.get(&dinv_, n));
+        ZV_TRY(keep.get(&didx, nnz));
+        ZV_TRY(keep.get(&dptr, n + 1));
+        ZV_TRY(keep.get(&dsrc, nnz));
+        ZV_TRY(keep.get(&ddpos, n));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(rows, order.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                                           st), "colouring: rows"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(dinv_, inv.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                                           st), "colouring: positions"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(didx, pidx.data(), nnz * sizeof(int),
+                                           cudaMemcpyHostToDevice, st), "colouring: columns"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(dptr, pptr.data(), (n + 1) * sizeof(long long),
+                                           cudaMemcpyHostToDevice, st), "colouring: row starts"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(dsrc, psrc.data(), nnz * sizeof(long long),
+                                           cudaMemcpyHostToDevice, st), "colouring: sources"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(ddpos, pdpos.data(), n * sizeof(long long),
+                                           cudaMemcpyHostToDevice, st), "colouring: diagonal"));
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colouring: upload"));
         v.gs_rows = rows;
-        return launch_status("node colouring");
+        v.pinv = dinv_;
+        v.pidx = didx;
+        v.pptr = dptr;
+        v.psrc = dsrc;
+        v.pdpos = ddpos;
+        return OK;
     }
 
     int build_structure() {
@@ -526,18 +582,24 @@ class Hierarchy {
             k_rows_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.rows); count_launch();
             if (prm.smoother == 1 && v.n > DENSE_MAX && (int)l < prm.gs_levels) {
                 if (l == 0 && coloured_indptr == v.indptr && coloured_n == v.n &&
-                    coloured_nnz == v.nnz && c0_rows) {
-                    v.gs_rows = c0_rows;                  // the finest pattern does not change
-                    v.gs_off = c0_off;
+                    coloured_nnz == v.nnz && c0.gs_rows) {
+                    // the finest pattern does not change: its colouring and colour order stay
+                    v.gs_rows = c0.gs_rows;
+                    v.gs_off = c0.gs_off;
+                    v.pptr = c0.pptr;
+                    v.pidx = c0.pidx;
+                    v.psrc = c0.psrc;
+                    v.pdpos = c0.pdpos;
+                    v.pinv = c0.pinv;
                 } else {
+                    if (l == 0) persist.release();
                     ZV_TRY(colour_level(v, l == 0 ? persist : structure));
                     scratch.release();
                     if (l == 0) {
                         coloured_indptr = v.indptr;
                         coloured_n = v.n;
                         coloured_nnz = v.nnz;
-                        c0_rows = v.gs_rows;
-                        c0_off = v.gs_off;
+                        c0 = v;
                     }
                 }
             }
@@ -565,6 +627,12 @@ class Hierarchy {
             k_narrow(perm, v.n, mem);
             v.mem = mem;
             v.mptr = seg;
+            if (v.pinv) {                      // the transfer in the colour order of the level
+                ZV_TRY(structure.get(&v.pagg, v.n));
+                ZV_TRY(structure.get(&v.pmem, v.n));
+                k_gather_int<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.gs_rows, v.agg, v.pagg); count_launch();
+                k_gather_int<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.mem, v.pinv, v.pmem); count_launch();
+            }
             // the Galerkin map: fine blocks grouped by (agg row, agg col)
             unsigned long long *gk;
             ZV_TRY(scratch.get(&gk, v.nnz));
@@ -606,6 +674,18 @@ class Hierarchy {
                 ZV_TRY(values.get(&v.data32, v.nnz * 16));
                 ZV_TRY(values.get(&v.dinv32, v.n * 16));
             }
+            if (v.pptr) {                      // the Gauss-Seidel levels' colour-ordered copy
+                if (prm.precision == 1) {
+                    ZV_TRY(values.get(&v.pdata32, v.nnz * 16));
+                    ZV_TRY(values.get(&v.pdinv32, v.n * 16));
+                } else {
+                    ZV_TRY(values.get(&v.pdata64, v.nnz * 16));
+                    ZV_TRY(values.get(&v.pdinv64, v.n * 16));
+                }
+                char *pb;
+                ZV_TRY(values.get(&pb, vs * v.n * 4));
+                v.pb = pb;
+            }
             if (v.dense) {
                 const size_t m = 4 * v.n;
                 ZV_TRY(values.get(&v.inv64, m * m));
@@ -625,10 +705,19 @@ class Hierarchy {
         for (size_t l = 0; l < L.size(); ++l) {
             Level &v = L[l];
             k_dinv<double><<<grid_for(v.n, 128), 128, 0, st>>>(v.n, v.data, v.dpos, v.dinv64); count_launch();
-            if (prm.precision == 1) {
-                k_convert<double, float><<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz * 16, v.data, v.data32); count_launch();
-                k_convert<double, float><<<grid_for(v.n * 16, 256), 256, 0, st>>>(v.n * 16, v.dinv64, v.dinv32); count_launch();
+            if (v.pptr) {
+                const unsigned gb = grid_for(v.nnz * 8, 256), gd = grid_for(v.n * 16, 256);
+                if (prm.precision == 1) {
+                    k_gather_blocks<float><<<gb, 256, 0, st>>>(v.nnz, v.psrc, v.data, v.pdata32); count_launch();
+                    k_permute_rows<true, double, float><<<gd, 256, 0, st>>>(v.n, 16, v.gs_rows, v.dinv64, v.pdinv32); count_launch();
+                } else {
+                    k_gather_blocks<double><<<gb, 256, 0, st>>>(v.nnz, v.psrc, v.data, v.pdata64); count_launch();
+                    k_permute_rows<true, double, double><<<gd, 256, 0, st>>>(v.n, 16, v.gs_rows, v.dinv64, v.pdinv64); count_launch();
+                }
             }
+            // FP32 copies in the original numbering: every level but the Gauss-Seidel ones
+            // (which sweep their colour-ordered copy), and those too once A^T is solved with
+            if (prm.precision == 1 && (!v.pptr || transposed_used)) ZV_TRY(convert_original(v));
             if (v.inv64) {
                 const int m = (int)(4 * v.n);
                 double *dense;
@@ -655,21 +744,15 @@ class Hierarchy {
         return launch_status("hierarchy values");
     }
 
+    int convert_original(Level &v) {
+        k_convert<double, float><<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz * 16, v.data, v.data32); count_launch();
+        k_convert<double, float><<<grid_for(v.n * 16, 256), 256, 0, st>>>(v.n * 16, v.dinv64, v.dinv32); count_launch();
+        return launch_status("fp32 copy");
+    }
+
     template <typename T, bool TRANS>
     int cycle(size_t l);
 };
-
-__global__ void k_colour_starts(const int *__restrict__ sorted, long long n, int C,
-                                long long *__restrict__ off) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c > C) return;
-    long long lo = 0, hi = n;
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        if (sorted[mid] < c) lo = mid + 1; else hi = mid;
-    }
-    off[c] = lo;
-}
 
 __global__ void k_iota_i32(int *p, long long n) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -732,7 +815,9 @@ void jacobi_t(int lanes, long long n, const Level &v, const V *data, const V *di
     }
 }
 
-// one Gauss-Seidel pass over the colours of level v, forward or backward (TRANS: on A^T)
+// one Gauss-Seidel pass over the colours of level v, forward or backward: on the colour-ordered
+// copy (data, dinv, b, x colour-ordered; each colour a contiguous row range), or with TRANS on
+// A^T in the original numbering (columns of A through the transpose structure, D^-T)
 template <bool TRANS, typename V, typename T>
 void gs_pass(const Level &v, const V *data, const V *dinv, const T *b, T *x, T omega, bool backward,
              cudaStream_t st) {
@@ -741,17 +826,17 @@ void gs_pass(const Level &v, const V *data, const V *dinv, const T *b, T *x, T o
         const int c = backward ? C - 1 - q : q;
         const long long o = v.gs_off[c], cnt = v.gs_off[c + 1] - v.gs_off[c];
         if (cnt <= 0) continue;
-        const int *rows = v.gs_rows + o;
         const int G = v.lanes;
         const unsigned grid = grid_for(cnt * G, 256);
         if (TRANS) {
+            const int *rows = v.gs_rows + o;
             if (G == 8) k_gs_colour_t<8, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
             else if (G == 16) k_gs_colour_t<16, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
             else k_gs_colour_t<32, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
         } else {
-            if (G == 8) k_gs_colour<8, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.indptr, v.indices, data, dinv, b, x, omega);
-            else if (G == 16) k_gs_colour<16, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.indptr, v.indices, data, dinv, b, x, omega);
-            else k_gs_colour<32, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.indptr, v.indices, data, dinv, b, x, omega);
+            if (G == 8) k_gs_colour<8, true, V, T><<<grid, 256, 0, st>>>(cnt, o, nullptr, v.pptr, v.pidx, data, dinv, b, x, omega);
+            else if (G == 16) k_gs_colour<16, true, V, T><<<grid, 256, 0, st>>>(cnt, o, nullptr, v.pptr, v.pidx, data, dinv, b, x, omega);
+            else k_gs_colour<32, true, V, T><<<grid, 256, 0, st>>>(cnt, o, nullptr, v.pptr, v.pidx, data, dinv, b, x, omega);
         }
         count_launch();
     }
@@ -764,12 +849,16 @@ struct CyclePick<double> {
     static const double *data(const Level &v) { return v.data; }
     static const double *dinv(const Level &v) { return v.dinv64; }
     static const double *inv(const Level &v) { return v.inv64; }
+    static const double *pdata(const Level &v) { return v.pdata64; }
+    static const double *pdinv(const Level &v) { return v.pdinv64; }
 };
 template <>
 struct CyclePick<float> {
     static const float *data(const Level &v) { return v.data32; }
     static const float *dinv(const Level &v) { return v.dinv32; }
     static const float *inv(const Level &v) { return v.inv32; }
+    static const float *pdata(const Level &v) { return v.pdata32; }
+    static const float *pdinv(const Level &v) { return v.pdinv32; }
 };
 
 // one V-cycle on level l: L[l].b -> L[l].x (zero initial guess); TRANS: the same cycle on
@@ -793,6 +882,33 @@ int Hierarchy::cycle(size_t l) {
     const bool last = (l + 1 == L.size()) || v.agg == nullptr;
     const int pre = last ? prm.coarse_sweeps : (jac_below ? prm.jacobi_sweeps : prm.presweeps);
     const int post = jac_below ? prm.jacobi_sweeps : prm.postsweeps;
+    if (gs_level && !TRANS) {
+        // sweeps, residual, restriction and prolongation on the colour-ordered copy; b comes
+        // in and x goes out in the level's own numbering
+        const V *pdata = CyclePick<T>::pdata(v);
+        const V *pdinv = CyclePick<T>::pdinv(v);
+        T *pb = static_cast<T *>(v.pb), *px = static_cast<T *>(v.x2), *pr = static_cast<T *>(v.r);
+        const unsigned g4 = grid_for(v.n * 4, 256);
+        k_permute_rows<true, T, T><<<g4, 256, 0, st>>>(v.n, 4, v.gs_rows, b, pb); count_launch();
+        cudaMemsetAsync(px, 0, v.n * 4 * sizeof(T), st);
+        auto sgs = [&](int sweeps) {      // symmetric: forward then backward over the colours
+            for (int s = 0; s < sweeps; ++s) {
+                gs_pass<false, V, T>(v, pdata, pdinv, pb, px, omega, false, st);
+                gs_pass<false, V, T>(v, pdata, pdinv, pb, px, omega, true, st);
+            }
+        };
+        sgs(pre);
+        if (!last) {
+            ZV_TRY((bsr_spmv_launch<true, V, T>(v.lanes, v.n, v.pptr, v.pidx, pdata, px, pb, pr, st)));
+            Level &c = L[l + 1];
+            k_restrict<T><<<grid_for(c.n * 4, 256), 256, 0, st>>>(c.n, v.mptr, v.pmem, pr, static_cast<T *>(c.b)); count_launch();
+            ZV_TRY((cycle<T, TRANS>(l + 1)));
+            k_prolong_add<T><<<g4, 256, 0, st>>>(v.n, v.pagg, static_cast<const T *>(c.x), px); count_launch();
+            sgs(prm.postsweeps);
+        }
+        k_permute_rows<false, T, T><<<g4, 256, 0, st>>>(v.n, 4, v.gs_rows, px, static_cast<T *>(v.x)); count_launch();
+        return launch_status(last ? "coarse smoothing" : "v-cycle");
+    }
     if (gs_level) {
         T *x = static_cast<T *>(v.x);
         auto sgs = [&](int sweeps) {      // symmetric: forward then backward over the colours
@@ -1002,6 +1118,7 @@ struct Solver {
         *iterations = it;
         *residual = res;
         *converged = res <= 1.01 * rt ? 1 : 0;
+        if (!trans) H.record_solve(it, *converged != 0);
         ZV_TRY(launch_status("fgmres"));
         return std::isfinite(res) ? OK : NON_FINITE;
     }
