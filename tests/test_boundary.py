@@ -47,3 +47,22 @@ def test_symmetry_and_pinned_pressure():
     np.testing.assert_array_equal(b.sym, o.sym)
     assert b.pin == o._pin
     np.testing.assert_array_equal(b.p_fixed, o.p_fixed)
+
+
+def test_union_of_meshes_offsets_nodes_elements_and_zones():
+    """The ensemble's disjoint union: node ranges, shifted connectivity and renumbered zones."""
+    from zvcfd_b200.ensemble import union
+    from zvcfd_b200.mesh import box, pipe
+
+    a = pipe(1e-3, 5e-3, n_core=4, n_ring=2, n_axial=6)
+    b = box((3, 3, 3), kind="tet")
+    m, off, ids = union([a, b])
+    assert list(off) == [0, a.n_nodes, a.n_nodes + b.n_nodes]
+    np.testing.assert_array_equal(m.nodes[off[1]:], b.nodes)
+    np.testing.assert_array_equal(m.elements["tet"][len(a.elements["tet"]):], b.elements["tet"] + off[1])
+    assert sorted(ids[0].values()) + sorted(ids[1].values()) == list(range(3, 3 + len(a.zones) + len(b.zones)))
+    for i, mesh in enumerate((a, b)):
+        for z, u in ids[i].items():
+            f, g = mesh.zones[z].faces, m.zones[u].faces
+            np.testing.assert_array_equal(g, np.where(f >= 0, f + off[i], -1))
+            assert m.zones[u].name.startswith(mesh.zones[z].name)

@@ -60,6 +60,7 @@ _SIGNATURES = {
     "zvfv_solver_solve": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_solve_t": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_vcycle": ([P, P, P, P], None),
+    "zvfv_solver_set_autotune": ([P, I32], None),
     "zvfv_solver_stats": ([P, I32, P, P, P], None),
     "zvfv_solver_level": ([P, I32, P, P, P, P, P], None),
     "zvfv_solver_destroy": ([P], None),

@@ -240,37 +240,31 @@ __global__ void k_seg_sum(long long nseg, int W, const long long *__restrict__ s
 }
 
 // The Galerkin sums of 4x4 blocks: dst[s] = sum of src[perm[q]] over q in [seg[s], seg[s+1]),
-// in that order (bit-equal to k_seg_sum with W = 16). Sixteen lanes own one coarse block: each
-// round the lanes fetch up to 16 of the segment's source indices at once, share them by
-// shuffle and issue all of their block loads before adding, so a segment of m blocks costs
-// ceil(m / 16) dependent round trips instead of 2 m.
+// in that order (bit-equal to k_seg_sum with W = 16). Sixteen lanes own one coarse block and
+// take the segment four entries at a time: the four source indices, then the four blocks'
+// entries, are loaded before any is added, so a segment (2-3 fine blocks on average) costs
+// two dependent round trips instead of two per entry.
 __global__ void __launch_bounds__(256)
 k_block_seg_sum(long long nseg, const long long *__restrict__ seg, const long long *__restrict__ perm,
                 const double *__restrict__ src, double *__restrict__ dst) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nseg * 16) return;
     const long long s = t / 16;
     const int c = (int)(t % 16);
-    const bool live = s < nseg;           // whole 16-lane groups share the fate of their segment
-    const long long q0 = live ? seg[s] : 0, q1 = live ? seg[s + 1] : 0;
-    // both halves of a warp run the same number of rounds, so every shuffle has all 32 lanes
-    long long rounds = (q1 - q0 + 15) / 16;
-    rounds = max(rounds, __shfl_xor_sync(0xffffffffu, rounds, 16));
+    const long long q1 = seg[s + 1];
     double acc = 0.0;
-    for (long long rd = 0; rd < rounds; ++rd) {
-        const long long base = q0 + rd * 16;
-        const int m = (int)max(0LL, min(16LL, q1 - base));
-        const long long mine = c < m ? __ldcs(perm + base + c) : 0;
-        double v[16];
+    for (long long q = seg[s]; q < q1; q += 4) {
+        long long p[4];
+        double v[4];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const long long pk = __shfl_sync(0xffffffffu, mine, k, 16);
-            v[k] = k < m ? __ldcs(src + pk * 16 + c) : 0.0;
-        }
+        for (int u = 0; u < 4; ++u) p[u] = q + u < q1 ? perm[q + u] : -1;
 #pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if (k < m) acc += v[k];
+        for (int u = 0; u < 4; ++u) v[u] = p[u] >= 0 ? __ldcs(src + p[u] * 16 + c) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (p[u] >= 0) acc += v[u];
     }
-    if (live) dst[t] = acc;
+    dst[t] = acc;
 }
 
 // inverse of every row's 4x4 diagonal block (Gauss-Jordan, partial pivoting); a singular
@@ -478,20 +472,23 @@ k_jacobi_t(long long n, const long long *__restrict__ tptr, const int *__restric
 // In-place block Gauss-Seidel over the rows of one colour (rows[0..count)): rows of a colour
 // are not coupled, so x_i <- x_i + omega D_i^-1 (b_i - (A x)_i) is a Jacobi step within the
 // colour and a Gauss-Seidel step across colours. A colour holds only a fraction of the rows,
-// so one launch is about one wave: each lane keeps GS_INFLIGHT blocks (and their column
-// indices) in flight before it uses them, instead of one dependent load after another.
-constexpr int GS_INFLIGHT = 4;
+// so one launch is a few waves at most and the sweep is latency-bound: each lane keeps
+// several blocks (and their column indices) in flight before it uses them, and the register
+// budget is held to 40 so that six 256-thread blocks fit on an SM (four FP32 blocks, or two
+// FP64 blocks, per lane fit in it without spilling).
+template <typename V>
+__host__ __device__ constexpr int gs_inflight() { return sizeof(V) == 4 ? 4 : 2; }
 
 // CONTIG: the colour is the contiguous row range [first, first + count) of a colour-ordered
 // copy (rows unused); otherwise its rows are rows[0..count) of the original numbering.
 template <int G, bool CONTIG, typename V, typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 6)
 k_gs_colour(long long count, long long first, const int *__restrict__ rows,
             const long long *__restrict__ indptr, const int *__restrict__ indices,
             const V *__restrict__ data, const V *__restrict__ dinv, const T *__restrict__ b,
             T *__restrict__ x, T omega) {
     constexpr int S = G / 4;
-    constexpr int U = GS_INFLIGHT;
+    constexpr int U = gs_inflight<V>();
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long k = gid / G;
     const int lane = threadIdx.x % G;
@@ -700,6 +697,7 @@ struct Params {
     int max_levels = 25;
     int rebuild_every = 0;   // > 0: re-aggregate every this many set-ups; 0: adaptively
     double rebuild_ratio = 1.5;   // adaptive: rebuild after a solve needing more iterations
+    int autotune = 0;        // 1: time each level's smoother at 8, 16 and 32 lanes per row
 };
 
 inline int lanes_for(long long n, long long nnz) {

@@ -83,13 +83,17 @@ k_arnoldi_pass(long long n, const double *__restrict__ V, long long ldv, int nv,
     }
 }
 
-// out[j] = sum over CTAs (in order) of partial[cta][j]
+// out[j] = sum over CTAs of partial[cta][j], one warp per column (launched with 32 * MAXV
+// threads): lane l adds the CTAs l, l + 32, ... in order, then a fixed butterfly adds the lanes,
+// so the result does not depend on scheduling. A single thread per column walking all CTAs
+// was a chain of several hundred dependent loads.
 __global__ void k_fold_cols(int ncta, int cols, const double *__restrict__ partial, double *__restrict__ out) {
-    const int j = threadIdx.x;
+    const int j = threadIdx.x / 32, lane = threadIdx.x % 32;
     if (j >= cols) return;
     double v = 0.0;
-    for (int c = 0; c < ncta; ++c) v += partial[(long long)c * MAXV + j];
-    out[j] = v;
+    for (int c = lane; c < ncta; c += 32) v += partial[(long long)c * MAXV + j];
+    v = warp_sum(v);
+    if (lane == 0) out[j] = v;
 }
 
 // partial dots of two vectors (a . b), MAXV-strided partials in column 0
@@ -269,7 +273,9 @@ class Hierarchy {
             L[0].indices = indices;
             for (size_t l = 1; l < L.size(); ++l) ZV_TRY(galerkin_values(l));
         }
-        return compute_values();
+        ZV_TRY(compute_values());
+        if (rebuild && prm.autotune) ZV_TRY(prm.precision == 1 ? autotune<float>() : autotune<double>());
+        return OK;
     }
 
     ~Hierarchy() {
@@ -752,6 +758,8 @@ class Hierarchy {
 
     template <typename T, bool TRANS>
     int cycle(size_t l);
+    template <typename T>
+    int autotune();
 };
 
 __global__ void k_iota_i32(int *p, long long n) {
@@ -966,6 +974,58 @@ int Hierarchy::cycle(size_t l) {
     return launch_status("v-cycle");
 }
 
+// The lanes-per-row autotuner: after each rebuild, every level of at least AUTOTUNE_MIN_ROWS
+// rows times one smoothing pass (a forward Gauss-Seidel pass over its colours, or a Jacobi
+// sweep) with 8, 16 and 32 lanes per row, twice each after a warm-up, with CUDA events on the
+// solver's stream, and keeps the fastest for all of that level's row kernels (smoothing,
+// residual). Different lanes add a row's blocks in a different order, so with the autotuner
+// on, two runs can differ in the last bits when their timings pick differently.
+constexpr long long AUTOTUNE_MIN_ROWS = 2048;
+
+template <typename T>
+int Hierarchy::autotune() {
+    using V = typename std::conditional<sizeof(T) == 4, float, double>::type;
+    cudaEvent_t e0, e1;
+    ZV_TRY(cuda_status(cudaEventCreate(&e0), "autotune event"));
+    ZV_TRY(cuda_status(cudaEventCreate(&e1), "autotune event"));
+    int rc = OK;
+    for (size_t l = 0; l < L.size() && rc == OK; ++l) {
+        Level &v = L[l];
+        if (v.dense || v.n < AUTOTUNE_MIN_ROWS) continue;
+        const bool gs = prm.smoother == 1 && !v.gs_off.empty();
+        const V *data = gs ? CyclePick<T>::pdata(v) : CyclePick<T>::data(v);
+        const V *dinv = gs ? CyclePick<T>::pdinv(v) : CyclePick<T>::dinv(v);
+        T *b = static_cast<T *>(gs ? v.pb : v.b), *x = static_cast<T *>(v.x2), *y = static_cast<T *>(v.x);
+        cudaMemsetAsync(b, 0, v.n * 4 * sizeof(T), st);
+        cudaMemsetAsync(x, 0, v.n * 4 * sizeof(T), st);
+        int best = v.lanes;
+        float best_ms = 1e30f;
+        for (int G : {8, 16, 32}) {
+            v.lanes = G;
+            float total = 0.0f;
+            for (int rep = 0; rep < 3 && rc == OK; ++rep) {
+                cudaEventRecord(e0, st);
+                if (gs) gs_pass<false, V, T>(v, data, dinv, b, x, (T)0.5, false, st);
+                else jacobi<false>(G, v.n, v.indptr, v.indices, data, dinv, b, x, y, (T)0.5, st);
+                cudaEventRecord(e1, st);
+                rc = cuda_status(cudaEventSynchronize(e1), "autotune");
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) total += ms;
+            }
+            if (total < best_ms) {
+                best_ms = total;
+                best = G;
+            }
+        }
+        v.lanes = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == OK) rc = launch_status("autotune");
+    return rc;
+}
+
 // ------------------------------------------------------------------ the solver handle
 
 struct Solver {
@@ -1042,7 +1102,7 @@ struct Solver {
 
     int dot2(const double *a, const double *b, double *out_dev) {
         k_dot_partial<<<ncta, DOT_THREADS, 0, st>>>(n4, a, b, partial); count_launch();
-        k_fold_cols<<<1, MAXV, 0, st>>>(ncta, 1, partial, out_dev); count_launch();
+        k_fold_cols<<<1, 32 * MAXV, 0, st>>>(ncta, 1, partial, out_dev); count_launch();
         return launch_status("dot");
     }
 
@@ -1088,11 +1148,11 @@ struct Solver {
                 ZV_TRY(apply(zk, nullptr, w, lr, trans));
                 const int nv = k + 1;
                 k_arnoldi_pass<0><<<ncta, DOT_THREADS, 0, st>>>(n4, V, n4, nv, nullptr, w, partial); count_launch();
-                k_fold_cols<<<1, MAXV, 0, st>>>(ncta, nv, partial, h1); count_launch();
+                k_fold_cols<<<1, 32 * MAXV, 0, st>>>(ncta, nv, partial, h1); count_launch();
                 k_arnoldi_pass<1><<<ncta, DOT_THREADS, 0, st>>>(n4, V, n4, nv, h1, w, partial); count_launch();
-                k_fold_cols<<<1, MAXV, 0, st>>>(ncta, nv, partial, h2); count_launch();
+                k_fold_cols<<<1, 32 * MAXV, 0, st>>>(ncta, nv, partial, h2); count_launch();
                 k_arnoldi_pass<2><<<ncta, DOT_THREADS, 0, st>>>(n4, V, n4, nv, h2, w, partial); count_launch();
-                k_fold_cols<<<1, MAXV, 0, st>>>(ncta, 1, partial, nrm); count_launch();
+                k_fold_cols<<<1, 32 * MAXV, 0, st>>>(ncta, 1, partial, nrm); count_launch();
                 k_arnoldi_finish<<<1, 1, 0, st>>>(k, ldh, h1, h2, nrm, Hm, cs, sn, g, stat); count_launch();
                 ZV_TRY(launch_status("arnoldi"));
                 cudaMemcpyAsync(host, stat, 3 * sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -1257,6 +1317,16 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream) {
 }
 
 // levels, and per level rows and blocks (arrays of max_levels entries)
+int zvfv_solver_set_autotune(void *handle, int on) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s) {
+        set_error("solver_set_autotune: no handle");
+        return BAD_ARGUMENT;
+    }
+    s->H.prm.autotune = on ? 1 : 0;
+    return OK;
+}
+
 int zvfv_solver_stats(void *handle, int max_levels, int *levels, int64_t *rows, int64_t *blocks) {
     Solver *s = static_cast<Solver *>(handle);
     if (!s) return BAD_ARGUMENT;

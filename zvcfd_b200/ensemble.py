@@ -1,0 +1,125 @@
+"""Batched solves: independent vessel problems assembled and solved as one system.
+
+The instances of an ensemble (meshes of uneven size, each with its own inlet flow and lumped
+outlets) share no nodes, so their union is one mesh whose coupled system is block diagonal.
+:class:`B200Ensemble` builds that union and runs one :class:`~zvcfd_b200.solver.B200Solver`
+on it: every stage of an outer iteration (gradients, element kernels per colour, the boundary
+pass, SpMV, the V-cycle graph, the Arnoldi passes, the update) is one launch over all
+instances instead of one per instance, the AMG aggregates never cross instances (they are
+not coupled), and the FGMRES basis holds every instance's residual at once. What stays per
+instance is the convergence test: an instance has converged when its own relative changes
+of velocity and pressure are below ``tol`` (the reference's criterion,
+``zvcfd/fv/solver.py:990-1005``, applied to its node range), and the ensemble stops when all
+have converged with the last linear solve converged.
+
+The reference solves instances one after the other; :func:`solve_sequentially` is that
+baseline on the same GPU.
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+
+from zvcfd_b200.mesh import Mesh, Zone
+from zvcfd_b200.solver import B200Solver
+from zvcfd_b200.topology import KINDS
+
+
+def union(meshes: list) -> tuple:
+    """The disjoint union of ``meshes``: ``(mesh, node_offsets (M+1,), zone_ids)`` where
+    ``zone_ids[i][z]`` is the union's id of zone ``z`` of instance ``i`` (ids from 3)."""
+    offsets = np.zeros(len(meshes) + 1, np.int64)
+    for i, m in enumerate(meshes):
+        offsets[i + 1] = offsets[i] + m.n_nodes
+    nodes = np.concatenate([m.nodes for m in meshes])
+    kinds = [k for k in KINDS if any(k in m.elements for m in meshes)]
+    elements = {k: np.concatenate([m.elements[k] + offsets[i] for i, m in enumerate(meshes)
+                                   if k in m.elements]) for k in kinds}
+    zones, ids, nxt = {}, [], 3
+    for i, m in enumerate(meshes):
+        ids.append({})
+        for z, zz in sorted(m.zones.items()):
+            f = np.where(zz.faces >= 0, zz.faces + offsets[i], -1)
+            zones[nxt] = Zone(nxt, zz.kind, f"{zz.name}#{i}", f)
+            ids[i][z] = nxt
+            nxt += 1
+    return Mesh(nodes, elements, zones), offsets, ids
+
+
+class B200Ensemble:
+    """Independent steady problems ``cases = [(mesh, bcs), ...]`` of one fluid, solved together
+    (see the module docstring). ``solver_options`` go to :class:`B200Solver`."""
+
+    def __init__(self, cases: list, fluid, **solver_options):
+        meshes = [m for m, _ in cases]
+        self.mesh, self.offsets, self.zone_ids = union(meshes)
+        bcs = {}
+        for i, (_, b) in enumerate(cases):
+            for z, spec in b.items():
+                bcs[self.zone_ids[i][z]] = spec
+        self.n = len(cases)
+        self.solver = B200Solver(self.mesh, fluid, bcs, **solver_options)
+        self._len = torch.as_tensor(np.diff(self.offsets), device="cuda")
+
+    def _per_instance(self, values, reduce):
+        return torch.segment_reduce(values, reduce, lengths=self._len)
+
+    def solve(self, *, max_iterations: int = 400, tol: float = 1e-8) -> dict:
+        """Outer iterations until every instance's relative changes are below ``tol``."""
+        s = self.solver
+        t0 = time.time()
+        done = np.zeros(self.n, bool)
+        first = np.full(self.n, -1)
+        hist = []
+        for it in range(max_iterations):
+            U0, P0 = s.U.clone(), s.P.clone()
+            rec = s.iterate()
+            du = self._per_instance((s.U - U0).abs().amax(1), "max")
+            um = self._per_instance(s.U.abs().amax(1), "max")
+            dp = self._per_instance((s.P - P0).abs(), "max")
+            pr = self._per_instance(s.P, "max") - self._per_instance(s.P, "min")
+            du = (du / um.clamp(min=1e-300)).cpu().numpy()
+            dp = (dp / pr.clamp(min=1e-300)).cpu().numpy()
+            ok = (du < tol) & (dp < tol) & (it > 0)
+            first[ok & (first < 0)] = it + 1
+            done = ok
+            hist.append({"iteration": it + 1, "du": du, "dp": dp,
+                         "linear_iterations": rec["linear_iterations"]})
+            if done.all() and rec["linear_converged"]:
+                break
+        return {"iterations": len(hist), "converged": bool(done.all()), "first_converged": first,
+                "history": hist, "seconds": time.time() - t0}
+
+    def fields(self, i: int) -> dict:
+        """Velocity and pressure of instance ``i``."""
+        a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+        f = self.solver.fields()
+        return {"U": f["U"][a:b], "P": f["P"][a:b]}
+
+    def patch_flows(self, i: int) -> dict:
+        """Volume outflow through each zone of instance ``i`` (its own zone ids)."""
+        q = self.solver.patch_flows()
+        return {z: q[u] for z, u in self.zone_ids[i].items()}
+
+    def close(self):
+        self.solver.close()
+
+
+def solve_sequentially(cases: list, fluid, *, max_iterations: int = 400, tol: float = 1e-8,
+                       **solver_options) -> dict:
+    """The baseline: each instance solved on its own, one after the other."""
+    t0 = time.time()
+    out = []
+    for m, bcs in cases:
+        s = B200Solver(m, fluid, bcs, **solver_options)
+        rep = s.solve(max_iterations=max_iterations, tol=tol)
+        out.append({"iterations": rep["iterations"], "converged": rep["converged"],
+                    "fields": s.fields(), "flows": s.patch_flows()})
+        s.close()
+    return {"instances": out, "seconds": time.time() - t0}
+
+
+__all__ = ["union", "B200Ensemble", "solve_sequentially"]
