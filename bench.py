@@ -12,6 +12,10 @@ independent replicas for N > 1: the path does not shard across GPUs). The matrix
 is larger than L2, so no flush is needed between steps.
 
 ``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]``
+
+Two further workloads print their own line (``--workload bifurcation``: the ~2M-node
+transient Y-bifurcation, mixed vs FP64 per BDF2 step; ``--workload ensemble``: 12 vessels
+solved together vs one after another); the default is the headline above.
 """
 
 from __future__ import annotations
@@ -33,6 +37,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "FV outer-iteration time & block-SpMV GB/s, mixed vs FP64 at 1e-8 rel. residual"
 UNIT = "outer-iterations/s"
 WORKLOAD = "curved Carreau-Yasuda tube, 400,686 nodes (hex core + 5 wedge wall layers), steady"
+# DRAM bytes per algorithmic byte of the FP64 block SpMV (k_bsr_spmv<16>): ncu measured
+# 696,748,032 B read + 5,399,808 B written for 703,481,132 algorithmic bytes on the 211,551-node
+# tube; the traffic of the full matrix is this ratio times its algorithmic bytes
+SPMV_TRAFFIC_PER_ALGORITHMIC_BYTE = (696_748_032 + 5_399_808) / 703_481_132
 
 
 def make_case(n_axial=285):
@@ -215,6 +223,122 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def bifurcation_workload(args):
+    """The mixed-precision transient workload: a seeded-tet Y-bifurcation of about 2M nodes
+    (parent radius 2 mm, daughters 1.6 and 1.4 mm at +-35 degrees, lengths 30/25/25 mm),
+    Newtonian blood, inlet Q(t) = 1 + 0.5 sin(2 pi t / 0.8) ml/s, RCR outlets Rp 1e8, C 1e-9,
+    Rd 1e9, BDF2 with dt 1e-3 and the reference's 5 coefficient loops per step. The FP32-
+    hierarchy solver and the FP64 solver march the same steps from the same steady state; the
+    field error of the mixed run against the FP64 run is reported at every step."""
+    import torch
+
+    from zvcfd_b200.fluid import Fluid
+    from zvcfd_b200.lumped import RCR
+    from zvcfd_b200.mesh import y_bifurcation
+    from zvcfd_b200.solver import B200Solver
+
+    h = 0.25e-3 * (56118.0 / args.nodes) ** (1.0 / 3.0)
+    t0 = time.perf_counter()
+    m = y_bifurcation(h, jitter_amount=0.05, seed=0)
+    gen = time.perf_counter() - t0
+    z = {zz.name: k for k, zz in m.zones.items()}
+
+    def Q(t):
+        return 1e-6 * (1.0 + 0.5 * np.sin(2 * np.pi * t / 0.8))
+
+    def shape(x):
+        return np.clip(1.0 - (x[:, 0] ** 2 + x[:, 1] ** 2) / 2e-3 ** 2, 0.0, None)
+
+    def bcs():
+        return {z["inlet"]: {"kind": "velocity", "flow_rate": Q, "profile": shape},
+                z["outlet1"]: {"kind": "pressure", "lumped": RCR(rp=1e8, c=1e-9, rd=1e9)},
+                z["outlet2"]: {"kind": "pressure", "lumped": RCR(rp=1e8, c=1e-9, rd=1e9)},
+                z["wall"]: {"kind": "wall"}}
+
+    fl = Fluid(1060.0, 3.5e-3)
+    runs = {}
+    for lin in ("b200", "b200-mixed"):
+        s = B200Solver(m, fl, bcs(), linear=lin, linear_rtol=0.1)
+        st = s.solve(max_iterations=400, tol=1e-8)
+        steps = []
+        for k in range(args.steps):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            rep = s.solve_transient(1e-3, 1, scheme="bdf2", loops=5, tol=1e-8)
+            torch.cuda.synchronize()
+            steps.append({"seconds": time.perf_counter() - t, "loops": rep["iterations"],
+                          "linear_iterations": sum(r["linear_iterations"] for r in rep["history"]),
+                          "fields": s.fields(), "flows": s.patch_flows()})
+        runs[lin] = {"steady_iterations": st["iterations"], "steps": steps}
+        s.close()
+    f64, mix = runs["b200"]["steps"], runs["b200-mixed"]["steps"]
+    err = []
+    for a, b in zip(f64, mix):
+        err.append({k: float(np.linalg.norm(b["fields"][k] - a["fields"][k]) /
+                             np.linalg.norm(a["fields"][k])) for k in ("U", "P")})
+    t64 = float(np.mean([x["seconds"] for x in f64[1:] or f64]))
+    tmx = float(np.mean([x["seconds"] for x in mix[1:] or mix]))
+    line = {"metric": "Y-bifurcation BDF2 time step (5 coefficient loops), mixed vs FP64",
+            "value": 1.0 / tmx, "unit": "time-steps/s", "n_gpus": 1, "steps": args.steps,
+            "higher_is_better": True, "dtype": "f64 (FGMRES) / f32 (hierarchy)",
+            "data": "synthetic",
+            "config": {"workload": f"Y-bifurcation, {m.n_nodes:,} nodes, "
+                                   f"{len(m.elements['tet']):,} seeded tets, lattice {h*1e3:.4f} mm",
+                       "dt": 1e-3, "loops": 5, "mesh_seconds": gen},
+            "fp64": {"seconds_per_step": t64, "steady_iterations": runs["b200"]["steady_iterations"],
+                     "linear_iterations": [x["linear_iterations"] for x in f64]},
+            "mixed": {"seconds_per_step": tmx, "speedup_vs_fp64": t64 / tmx,
+                      "linear_iterations": [x["linear_iterations"] for x in mix],
+                      "field_error_vs_fp64_per_step": err},
+            "outlet_flows_ml_s": [{str(k): v * 1e6 for k, v in x["flows"].items()} for x in mix]}
+    print(json.dumps(line), flush=True)
+
+
+def ensemble_workload(args):
+    """The batched-ensemble workload: 12 seeded vessels of log-uniform sizes in 50k-1.2M nodes
+    (straight, curved, bifurcating in turn), random inlet flows and RCR outlets, steady to
+    1e-8; the instances solved one after another in plain FP64 against all of them solved
+    together with the FP32 hierarchy and the lanes autotuner."""
+    import torch
+
+    from zvcfd_b200.ensemble import B200Ensemble, solve_sequentially, synthetic_ensemble
+    from zvcfd_b200.fluid import Fluid
+
+    t0 = time.perf_counter()
+    cases = synthetic_ensemble(count=args.instances, seed=0)
+    gen = time.perf_counter() - t0
+    fl = Fluid(1060.0, 3.5e-3)
+    torch.cuda.synchronize()
+    seq = solve_sequentially(cases, fl, tol=1e-8, max_iterations=400, linear="b200")
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    ens = B200Ensemble(cases, fl, linear="b200-mixed", linear_options={"autotune": True})
+    rep = ens.solve(tol=1e-8, max_iterations=400)
+    torch.cuda.synchronize()
+    t_ens = time.perf_counter() - t
+    err = []
+    for i, r in enumerate(seq["instances"]):
+        f = ens.fields(i)
+        err.append(max(float(np.linalg.norm(f[k] - r["fields"][k]) / np.linalg.norm(r["fields"][k]))
+                       for k in ("U", "P")))
+    ens.close()
+    sizes = [m.n_nodes for m, _ in cases]
+    line = {"metric": "batched ensemble solves/s vs sequential FP64", "value": len(cases) / t_ens,
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "dtype": "f64 (FGMRES) / f32 (hierarchy)",
+            "config": {"workload": f"{len(cases)} vessels, {sum(sizes):,} nodes in all",
+                       "nodes": sizes, "tol": 1e-8, "mesh_seconds": gen},
+            "sequential_fp64": {"value": len(cases) / seq["seconds"], "seconds": seq["seconds"],
+                                "outer_iterations": [r["iterations"] for r in seq["instances"]],
+                                "converged": all(r["converged"] for r in seq["instances"])},
+            "batched_mixed": {"seconds": t_ens, "outer_iterations": rep["iterations"],
+                              "converged": rep["converged"],
+                              "first_converged": [int(x) for x in rep["first_converged"]],
+                              "field_error_vs_sequential": err},
+            "speedup": seq["seconds"] / t_ens}
+    print(json.dumps(line), flush=True)
+
+
 def max_over_ranks(value, dist, device):
     """The largest of every rank's ``value`` (the job's time is its slowest replica's)."""
     import torch
@@ -245,6 +369,11 @@ def main():
     ap.add_argument("--cpu-axial", type=int, default=3, help="axial cells of the CPU sample")
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="tube", choices=["tube", "bifurcation", "ensemble"],
+                    help="tube: the headline (default); bifurcation: the ~2M-node transient "
+                         "Y-bifurcation; ensemble: 12 vessels solved together vs one by one")
+    ap.add_argument("--nodes", type=int, default=2_000_000, help="bifurcation workload size")
+    ap.add_argument("--instances", type=int, default=12, help="ensemble workload size")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark the timed steps with an NVTX range 'timed' (for ncu --nvtx-include)")
     args = ap.parse_args()
@@ -254,6 +383,13 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workload != "tube":
+        import torch
+
+        torch.cuda.set_device(local)
+        if rank == 0:
+            (bifurcation_workload if args.workload == "bifurcation" else ensemble_workload)(args)
+        return
 
     import torch
 
@@ -322,7 +458,11 @@ def main():
             "peak": peak, "unit": "GB/s", "frac": sp["fp64"]["gbs"] / peak,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6.65 TB/s",
-            "algorithmic_bytes": sp["fp64"]["bytes"], "traffic": None}
+            "algorithmic_bytes": sp["fp64"]["bytes"],
+            "traffic": SPMV_TRAFFIC_PER_ALGORITHMIC_BYTE * sp["fp64"]["bytes"],
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel "
+                              "on the 211,551-node tube (5,214,011 blocks, larger than L2), scaled "
+                              "by algorithmic bytes (profiles/k_bsr_spmv_fp64_curved_tube.txt)"}
     extra["spmv"] = {"fp64_gbs": sp["fp64"]["gbs"], "fp32_gbs": sp["fp32"]["gbs"],
                      "fp64_us": sp["fp64"]["seconds"] * 1e6, "fp32_us": sp["fp32"]["seconds"] * 1e6,
                      "nnzb": nnzb, "rows": n}

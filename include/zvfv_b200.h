@@ -240,11 +240,16 @@ int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, i
                         double *residual, int *converged, void *stream);
 /* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:386-399) */
 int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
-/* Lanes-per-row autotuning of the hierarchy (off by default): after each rebuild, every level
- * of 2048 rows or more times one smoothing pass at 8, 16 and 32 lanes per row and keeps the
- * fastest. The reference has no counterpart (AmgX fixes its kernels' shapes); the batched
- * ensemble workload turns it on. With it on, runs can differ in the last bits. */
-int zvfv_solver_set_autotune(void *handle, int on);
+/* Hierarchy options beyond create (each takes effect at the next set-up, which rebuilds):
+ *   "autotune" (0/1, default 0): after each rebuild, every level of 2048 rows or more times one
+ *       smoothing pass at 8, 16 and 32 lanes per row and keeps the fastest (AmgX fixes its
+ *       kernels' shapes; no reference counterpart); runs can then differ in the last bits;
+ *   "gs_levels" (default 2): the finest levels smoothed by Gauss-Seidel, Jacobi below;
+ *   "jacobi_sweeps" (default 2), "jacobi_omega" (default 0.7): the block-Jacobi smoothing of
+ *       the levels below (the reference ACM's damped Jacobi, zvcfd/fv/linear.py:343, :480-502);
+ *   "rebuild_ratio" (default 1.5): the adaptive rebuild threshold.
+ * Unknown names or out-of-range values return ZVFV_BAD_ARGUMENT. */
+int zvfv_solver_set_option(void *handle, const char *name, double value);
 /* hierarchy sizes (ACM.stats, zvcfd/fv/linear.py:513-518) */
 int zvfv_solver_stats(void *handle, int max_levels, int *levels, int64_t *rows, int64_t *blocks);
 /* one level's size and aggregates (agg: n int32 entries, or NULL) */

@@ -60,7 +60,7 @@ _SIGNATURES = {
     "zvfv_solver_solve": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_solve_t": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_vcycle": ([P, P, P, P], None),
-    "zvfv_solver_set_autotune": ([P, I32], None),
+    "zvfv_solver_set_option": ([P, ctypes.c_char_p, F64], None),
     "zvfv_solver_stats": ([P, I32, P, P, P], None),
     "zvfv_solver_level": ([P, I32, P, P, P, P, P], None),
     "zvfv_solver_destroy": ([P], None),

@@ -321,6 +321,7 @@ class Hierarchy {
     // the iterations of the first solve after the last rebuild (and at least 2 more).
     bool rebuild_requested = false;
     int base_iterations = -1;
+    void request_rebuild() { rebuild_requested = true; }
     void record_solve(int iterations, bool converged) {
         if (prm.rebuild_every > 0) return;
         if (base_iterations < 0) {
@@ -1317,13 +1318,24 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream) {
 }
 
 // levels, and per level rows and blocks (arrays of max_levels entries)
-int zvfv_solver_set_autotune(void *handle, int on) {
+int zvfv_solver_set_option(void *handle, const char *name, double value) {
     Solver *s = static_cast<Solver *>(handle);
-    if (!s) {
-        set_error("solver_set_autotune: no handle");
+    if (!s || !name) {
+        set_error("solver_set_option: no handle or name");
         return BAD_ARGUMENT;
     }
-    s->H.prm.autotune = on ? 1 : 0;
+    Params &p = s->H.prm;
+    const std::string opt(name);
+    if (opt == "autotune") p.autotune = value != 0.0 ? 1 : 0;
+    else if (opt == "gs_levels" && value >= 0) p.gs_levels = (int)value;
+    else if (opt == "jacobi_sweeps" && value >= 1) p.jacobi_sweeps = (int)value;
+    else if (opt == "jacobi_omega" && value > 0) p.jacobi_omega = value;
+    else if (opt == "rebuild_ratio" && value >= 1) p.rebuild_ratio = value;
+    else {
+        set_error("solver_set_option: unknown option or bad value: %s = %g", name, value);
+        return BAD_ARGUMENT;
+    }
+    s->H.request_rebuild();                  // the next set-up builds with the new setting
     return OK;
 }
 

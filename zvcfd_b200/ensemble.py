@@ -122,4 +122,64 @@ def solve_sequentially(cases: list, fluid, *, max_iterations: int = 400, tol: fl
     return {"instances": out, "seconds": time.time() - t0}
 
 
-__all__ = ["union", "B200Ensemble", "solve_sequentially"]
+def _section_nodes(radius, n_core, n_ring, growth):
+    from zvcfd_b200.mesh import ogrid_section
+
+    return len(ogrid_section(radius, n_core, n_ring, growth=growth)[0])
+
+
+def vessel(kind: str, nodes: int, seed: int):
+    """A seeded vessel mesh of about ``nodes`` nodes: ``"straight"`` (the tet pipe of the
+    Poiseuille workload, radius 1 mm, length 10 mm), ``"curved"`` (the hexahedral/prismatic
+    90-degree tube, radius 2 mm, bend 20 mm) or ``"bifurcating"`` (the tet Y-bifurcation).
+    Returns ``(mesh, inlet radius, outlet zone names)``."""
+    from zvcfd_b200.mesh import curved_tube, pipe, y_bifurcation
+
+    if kind == "straight":
+        k = (nodes / 49977.0) ** (1.0 / 3.0)
+        nc, nr = max(3, round(14 * k)), max(2, round(7 * k))
+        P = _section_nodes(1e-3, nc, nr, 1.0)
+        return (pipe(1e-3, 10e-3, n_core=nc, n_ring=nr, n_axial=max(4, round(nodes / P) - 1),
+                     kind="tet", jitter_amount=0.05, seed=seed), 1e-3, ["outlet"])
+    if kind == "curved":
+        k = (nodes / 400686.0) ** (1.0 / 3.0)
+        nc, nr = max(4, round(20 * k)), max(6, round(12 * k))
+        P = _section_nodes(2e-3, nc, nr, 0.8)
+        return (curved_tube(2e-3, 20e-3, np.pi / 2, n_core=nc, n_ring=nr,
+                            n_axial=max(4, round(nodes / P) - 1), layers=5, growth=0.8), 2e-3,
+                ["outlet"])
+    if kind == "bifurcating":
+        h = 0.25e-3 * (56118.0 / nodes) ** (1.0 / 3.0)
+        return y_bifurcation(h, jitter_amount=0.05, seed=seed), 2e-3, ["outlet1", "outlet2"]
+    raise ValueError(f"vessel kind {kind!r}")
+
+
+def synthetic_ensemble(count: int = 12, low: int = 50_000, high: int = 1_200_000, seed: int = 0):
+    """The batched-ensemble workload: ``count`` vessels of log-uniform sizes in
+    ``[low, high]`` nodes, kinds in turn straight / curved / bifurcating, each with a
+    parabolic inlet of flow U(0.5, 3) ml/s and RCR outlets with log-uniform
+    Rp in [0.5, 2]e8, C in [0.5, 2]e-9, Rd in [0.5, 2]e9 (SI). Returns ``[(mesh, bcs)]``."""
+    from zvcfd_b200.lumped import RCR
+
+    rng = np.random.default_rng(seed)
+    kinds = ("straight", "curved", "bifurcating")
+    cases = []
+    for i in range(count):
+        target = int(np.exp(rng.uniform(np.log(low), np.log(high))))
+        m, R, outlets = vessel(kinds[i % 3], target, seed + i)
+        z = {zz.name: k for k, zz in m.zones.items()}
+        q = rng.uniform(0.5e-6, 3e-6)
+
+        def shape(x, R=R):
+            return np.clip(1.0 - (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2, 0.0, None)
+
+        bcs = {z["inlet"]: {"kind": "velocity", "flow_rate": q, "profile": shape},
+               z["wall"]: {"kind": "wall"}}
+        for name in outlets:
+            rp, c, rd = np.exp(rng.uniform(np.log(0.5), np.log(2.0), 3)) * np.array([1e8, 1e-9, 1e9])
+            bcs[z[name]] = {"kind": "pressure", "lumped": RCR(rp=rp, c=c, rd=rd)}
+        cases.append((m, bcs))
+    return cases
+
+
+__all__ = ["union", "B200Ensemble", "solve_sequentially", "vessel", "synthetic_ensemble"]
