@@ -305,7 +305,7 @@ def ensemble_workload(args):
     from zvcfd_b200.fluid import Fluid
 
     t0 = time.perf_counter()
-    cases = synthetic_ensemble(count=args.instances, seed=0)
+    cases = synthetic_ensemble(count=args.instances, high=args.max_nodes, seed=0)
     gen = time.perf_counter() - t0
     fl = Fluid(1060.0, 3.5e-3)
     torch.cuda.synchronize()
@@ -374,6 +374,8 @@ def main():
                          "Y-bifurcation; ensemble: 12 vessels solved together vs one by one")
     ap.add_argument("--nodes", type=int, default=2_000_000, help="bifurcation workload size")
     ap.add_argument("--instances", type=int, default=12, help="ensemble workload size")
+    ap.add_argument("--max-nodes", type=int, default=1_200_000,
+                    help="ensemble workload: largest instance (log-uniform from 50,000)")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark the timed steps with an NVTX range 'timed' (for ncu --nvtx-include)")
     args = ap.parse_args()

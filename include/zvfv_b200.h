@@ -133,6 +133,19 @@ int zvfv_massflow(int kind, int stored, const int32_t *conn, int n_colours,
                   const double *snode, int nlev, double c1, const double *Uo1, const double *mo1,
                   double c2, const double *Uo2, const double *mo2, double rho, double *mdot,
                   double *imbalance, double *adv, void *stream);
+/* zvfv_massflow plus, in the same element pass, the viscous part of the next momentum
+ * diagonal from the same velocity (the terms of zvfv_diagonal without the advective part,
+ * which adv already holds): the next iteration's a_P = vdiag + adv (accumulated into vdiag,
+ * N). No reference counterpart: the reference launches its diag kernel separately
+ * (zvcfd/fv/_cuda_fast.py:239-299). */
+int zvfv_massflow_diag(int kind, int stored, const int32_t *conn, int n_colours,
+                       const int64_t *colour_offsets, const double *X, const double *geo,
+                       const double *U, const double *P, const double *gradP, const double *dnode,
+                       const double *snode, int nlev, double c1, const double *Uo1,
+                       const double *mo1, double c2, const double *Uo2, const double *mo2,
+                       double rho, int rheo, double mu0, double muinf, double lam, double ca,
+                       double cn, int transpose, int has_mut, const double *mut, double *mdot,
+                       double *imbalance, double *adv, double *vdiag, void *stream);
 
 /* Boundary rows, raw-row copy, Dirichlet with symmetric elimination, residual partials and
  * dimensionless row scaling (kernel finalise, zvcfd/fv/_cuda_bc.py:32-138, launched at
@@ -211,10 +224,13 @@ int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const i
  * zvcfd/fv/linear.py:728-739, :846-868, :905-955) and its own ACM (linear.py:328-518).
  * create: precision 0 FP64, 1 FP32 hierarchy; smoother 0 damped block Jacobi, 1 symmetric
  * multicolour block Gauss-Seidel (AmgX's MULTICOLOR_GS of the `gs` preset, linear.py:76-79);
- * strength 0 block norm, 1 pressure entry. rebuild_every > 0 re-aggregates every that many
+ * strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
+ * directions of each coupling (the default of the Python back end: convection otherwise
+ * stalls the pairwise matching). rebuild_every > 0 re-aggregates every that many
  * set-ups (the reference's ACM, linear.py:337-348); 0 keeps the aggregates until a solve fails
- * or needs more than 1.5 times (and 2 more than) the iterations of the first solve after the
- * last rebuild (the reuse policy of its AmgX binding, linear.py:686-698, :837-841). */
+ * or needs more than 1.5 times (and 2 more than) the most iterations of the first three solves
+ * after the last rebuild (after the reuse policy of its AmgX binding, linear.py:686-698,
+ * :837-841, which takes the first solve alone). */
 int zvfv_solver_create(void **handle, int precision, int smoother, int strength, int passes,
                        int presweeps, int postsweeps, double omega, int coarse_sweeps,
                        int max_levels, int rebuild_every, int restart);
@@ -250,6 +266,8 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
  *   "rebuild_ratio" (default 1.5): the adaptive rebuild threshold.
  * Unknown names or out-of-range values return ZVFV_BAD_ARGUMENT. */
 int zvfv_solver_set_option(void *handle, const char *name, double value);
+/* The value of an option above, or a counter: "rebuilds" (hierarchy builds so far), "setups". */
+int zvfv_solver_get_option(void *handle, const char *name, double *value);
 /* hierarchy sizes (ACM.stats, zvcfd/fv/linear.py:513-518) */
 int zvfv_solver_stats(void *handle, int max_levels, int *levels, int64_t *rows, int64_t *blocks);
 /* one level's size and aggregates (agg: n int32 entries, or NULL) */

@@ -85,13 +85,27 @@ def pairwise(n, indptr, indices, strength):
     return agg, nxt
 
 
-def aggregate(indptr, indices, data, passes=2, mode=0):
-    """``passes`` pairwise passes with the graph coarsened between them by summing strengths
-    per aggregate pair (``zvcfd/fv/linear.py:415-433``). Returns ``(agg, count)``."""
+def transpose_positions(indptr, indices):
+    """Position of the entry (j, i) for every entry (i, j) of a structurally symmetric pattern."""
     n = len(indptr) - 1
     rows = np.repeat(np.arange(n), np.diff(indptr))
     cols = np.asarray(indices, np.int64)
-    w = block_weights(data, mode)
+    order = np.lexsort((rows, cols))          # entries by (column, row): the transpose's order
+    pos = np.empty(len(cols), np.int64)
+    pos[order] = np.arange(len(cols))
+    return pos
+
+
+def aggregate(indptr, indices, data, passes=2, mode=0):
+    """``passes`` pairwise passes with the graph coarsened between them by summing strengths
+    per aggregate pair (``zvcfd/fv/linear.py:415-433``). Returns ``(agg, count)``. ``mode`` 2
+    (not in the reference) averages each block norm with that of its transpose position."""
+    n = len(indptr) - 1
+    rows = np.repeat(np.arange(n), np.diff(indptr))
+    cols = np.asarray(indices, np.int64)
+    w = block_weights(data, 1 if mode == 1 else 0)
+    if mode == 2:
+        w = 0.5 * (w + w[transpose_positions(indptr, indices)])
     total = np.arange(n)
     count = n
     ptr = np.asarray(indptr, np.int64)

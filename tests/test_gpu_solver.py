@@ -30,7 +30,7 @@ def _system(name="pipe_tet_si", iterations=3):
     return s, A, b.reshape(-1).clone(), x0
 
 
-@pytest.mark.parametrize("strength", ["block", "pressure"])
+@pytest.mark.parametrize("strength", ["symmetric", "block", "pressure"])
 def test_aggregation_is_bit_exact(strength):
     from zvcfd_b200.linear import B200AMG
 
@@ -39,7 +39,7 @@ def test_aggregation_is_bit_exact(strength):
     solver.setup(A)
     ip, ix = A.indptr.cpu().numpy(), A.indices.cpu().numpy()
     data = A.data.cpu().numpy()
-    mode = 1 if strength == "pressure" else 0
+    mode = {"block": 0, "pressure": 1, "symmetric": 2}[strength]
     level = 0
     while True:
         n, nnz, nc, agg = solver.level(level, with_aggregates=True)

@@ -39,6 +39,8 @@ _SIGNATURES = {
                        F64, I32, F64, F64, F64, F64, F64, I32, I32, I32, P, P, P, P, P, P], None),
     "zvfv_massflow": ([I32, I32, P, I32, P, P, P, P, P, P, P, P, I32, F64, P, P, F64, P, P, F64,
                        P, P, P, P], None),
+    "zvfv_massflow_diag": ([I32, I32, P, I32, P, P, P, P, P, P, P, P, I32, F64, P, P, F64, P, P,
+                            F64, I32, F64, F64, F64, F64, F64, I32, I32, P, P, P, P, P, P], None),
     "zvfv_limiter": ([I32, I32, P, I32, P, P, P, P, P, P, P, P, P], None),
     "zvfv_gradient": ([I64, I32, I32, P, P, P, P, P, P, P], None),
     "zvfv_minmax": ([I64, P, P, P, P, P, P], None),
@@ -61,6 +63,7 @@ _SIGNATURES = {
     "zvfv_solver_solve_t": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_vcycle": ([P, P, P, P], None),
     "zvfv_solver_set_option": ([P, ctypes.c_char_p, F64], None),
+    "zvfv_solver_get_option": ([P, ctypes.c_char_p, P], None),
     "zvfv_solver_stats": ([P, I32, P, P, P], None),
     "zvfv_solver_level": ([P, I32, P, P, P, P, P], None),
     "zvfv_solver_destroy": ([P], None),

@@ -248,19 +248,28 @@ class B200Assembler:
                  ptr(K.pos), ptr(data), ptr(b), st)
         return data.view(-1, 4, 4), b.view(self.N, 4)
 
-    def massflow(self, U, P, gradP, dnode, snode, *, levels=(), out=None):
-        """``(mdot {kind: (E, n_ip)} slot order, net outflow (N,), advective diagonal (N,))``."""
+    def massflow(self, U, P, gradP, dnode, snode, *, levels=(), out=None, vdiag=None,
+                 mu_t=None):
+        """``(mdot {kind: (E, n_ip)} slot order, net outflow (N,), advective diagonal (N,))``.
+        With ``vdiag`` (N,), the same element pass also accumulates into it the viscous part
+        of the next momentum diagonal from ``U`` (``diagonal`` without its advective part)."""
         imb = torch.zeros(self.N, dtype=torch.float64, device=self.device)
         adv = torch.zeros(self.N, dtype=torch.float64, device=self.device)
         res = {}
         U_, P_, gP, dn, sn = (self._vec(a) for a in (U, P, gradP, dnode, snode))
         st = stream_ptr()
+        hm, mt = self._mut(mu_t)
         for K in self.kinds:
             m = torch.empty((K.E, K.nip), dtype=torch.float64, device=self.device) \
                 if out is None else out[K.kind]
-            call("zvfv_massflow", K.code, int(K.stored), ptr(K.conn), K.n_colours,
-                 K.host_offsets, ptr(self.X), ptr(K.geo), ptr(U_), ptr(P_), ptr(gP), ptr(dn),
-                 ptr(sn), *self._levels(levels, K.kind), self.rho, ptr(m), ptr(imb), ptr(adv), st)
+            head = (K.code, int(K.stored), ptr(K.conn), K.n_colours, K.host_offsets,
+                    ptr(self.X), ptr(K.geo), ptr(U_), ptr(P_), ptr(gP), ptr(dn), ptr(sn),
+                    *self._levels(levels, K.kind), self.rho)
+            if vdiag is None:
+                call("zvfv_massflow", *head, ptr(m), ptr(imb), ptr(adv), st)
+            else:
+                call("zvfv_massflow_diag", *head, *self.rheo, self.transpose, hm, mt, ptr(m),
+                     ptr(imb), ptr(adv), ptr(vdiag), st)
             res[K.kind] = m
         return res, imb, adv
 

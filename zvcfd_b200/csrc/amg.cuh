@@ -63,6 +63,17 @@ __global__ void k_block_weight(long long nnz, const double *__restrict__ data, i
     w[p] = sqrt(s);
 }
 
+// symmetrised coupling weights: ws[p] = (w[p] + w[p^T]) / 2 with p^T the entry (j, i) of the
+// entry p = (i, j). On a symmetric pattern with sorted rows, the transpose's q-th entry is the
+// entry q of A itself and holds A's block tperm[q], so p^T of tperm[q] is q.
+__global__ void k_symmetric_weight(long long nnz, const long long *__restrict__ tperm,
+                                   const double *__restrict__ w, double *__restrict__ ws) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nnz) return;
+    const long long p = tperm[q];
+    ws[p] = 0.5 * (w[p] + w[q]);
+}
+
 // row of every entry (CSR)
 __global__ void k_rows_of(long long n, const long long *__restrict__ indptr, long long *__restrict__ row) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -689,7 +700,7 @@ struct Params {
     int gs_levels = 2;       // with Gauss-Seidel: the finest levels that use it (Jacobi below)
     int jacobi_sweeps = 2;   // damped block-Jacobi sweeps (pre and post) below them
     double jacobi_omega = 0.7;
-    int strength = 0;        // 0 block norm, 1 pressure-pressure entry
+    int strength = 2;        // 0 block norm, 1 pressure-pressure entry, 2 symmetrised block norm
     int passes = 2;
     int presweeps = 2, postsweeps = 2;
     double omega = 0.7;

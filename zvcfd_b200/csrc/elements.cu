@@ -401,11 +401,20 @@ struct MassArgs {
     const double *Uo2, *mo2;
     double rho;
     double *mdot, *imbalance, *adv;
+    // VDIAG: the viscous part of the next momentum diagonal from the same (new) velocity
+    Rheology rh;
+    int transpose, has_mut;
+    const double *mut;
+    double *vdiag;
 };
 
 // New Rhie-Chow mass flows, each node's net interior outflow and the advective part of the
-// next momentum diagonal (zvcfd/fv/_cuda_fast.py:469-553; reference.py:922-948)
-template <int K, bool STORED>
+// next momentum diagonal (zvcfd/fv/_cuda_fast.py:469-553; reference.py:922-948). With VDIAG the
+// same pass adds the viscous part of the next diagonal (the terms of k_diag,
+// zvcfd/fv/_cuda_fast.py:239-299), so that the next iteration's a_P = vdiag + adv needs no
+// element pass of its own: the velocity and mass flows k_diag would read at the start of that
+// iteration are the ones at hand here.
+template <int K, bool STORED, bool VDIAG>
 __global__ void __launch_bounds__(threads_of<K>(), ELEMENT_MIN_BLOCKS)
 k_massflow(const MassArgs g, long long base, long long count) {
     using T = Topo<K>;
@@ -422,6 +431,7 @@ k_massflow(const MassArgs g, long long base, long long count) {
     __shared__ double s_sn[T::EPB][N];
     __shared__ double s_rec[T::EPB][T::REC];
     __shared__ double s_m[T::EPB][T::NIP];
+    __shared__ double s_mu[VDIAG ? T::EPB : 1][VDIAG ? T::NIP : 1];
     __shared__ int s_n[T::EPB][N];
     __shared__ SmemTab<K> tab;
     tab.load();
@@ -470,20 +480,44 @@ k_massflow(const MassArgs g, long long base, long long count) {
         }
         g.mdot[slot * T::NIP + s] = m;
         s_m[le][s] = m;
+        if (VDIAG) {
+            double mu = g.rh.mu0;
+            if (g.rh.model) {
+                double gu[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                for (int q = 0; q < N; ++q) {
+                    const double *G = R::G(rec, s, q);
+                    for (int j = 0; j < 3; ++j)
+                        for (int k = 0; k < 3; ++k) gu[j][k] += s_u[le][q * 3 + j] * G[k];
+                }
+                mu = viscosity(gu, g.rh);
+            }
+            if (g.has_mut)
+                for (int q = 0; q < N; ++q) mu += tab.nip[s][q] * g.mut[s_n[le][q]];
+            s_mu[le][s] = mu;
+        }
     }
     __syncthreads();
     if (!active || t >= N) return;
     const int a = t;
-    double out = 0.0, ad = 0.0;
+    double out = 0.0, ad = 0.0, vd = 0.0;
     for (int i = 0; i < MAXI; ++i) {
         const int s = tab.ips[a][i];
         if (s < 0) break;
         const double sg = tab.sgn[a][i], m = s_m[le][s];
         out += sg * m;
         ad += sg > 0 ? fmax(m, 0.0) : fmax(-m, 0.0);
+        if (VDIAG) {
+            const double mu = s_mu[le][s];
+            const double *A = R::A(rec, s);
+            const double *G = R::G(rec, s, a);
+            double r = -mu * (G[0] * A[0] + G[1] * A[1] + G[2] * A[2]);
+            if (g.transpose) r -= mu * G[0] * A[0];
+            vd += sg * r;
+        }
     }
     g.imbalance[s_n[le][a]] += out;
     g.adv[s_n[le][a]] += ad;
+    if (VDIAG) g.vdiag[s_n[le][a]] += vd;
 }
 
 // --------------------------------------------------------------------------- limiter
@@ -605,10 +639,13 @@ struct AssembleL {
 template <int K, bool S>
 struct MassL {
     static int run(const MassArgs &g, int nc, const int64_t *off, cudaStream_t st) {
-        static const bool carveout = (prefer_shared(k_massflow<K, S>), true);
+        static const bool carveout = (prefer_shared(k_massflow<K, S, false>),
+                                      prefer_shared(k_massflow<K, S, true>), true);
         (void)carveout;
         per_colour<K>(nc, off, [&](unsigned grid, long long base, long long count) {
-            k_massflow<K, S><<<grid, threads_of<K>(), 0, st>>>(g, base, count); count_launch();
+            if (g.vdiag) k_massflow<K, S, true><<<grid, threads_of<K>(), 0, st>>>(g, base, count);
+            else k_massflow<K, S, false><<<grid, threads_of<K>(), 0, st>>>(g, base, count);
+            count_launch();
         });
         return launch_status("massflow");
     }
@@ -728,7 +765,26 @@ int zvfv_massflow(int kind, int stored, const int32_t *conn, int n_colours,
                   double c2, const double *Uo2, const double *mo2, double rho, double *mdot,
                   double *imbalance, double *adv, void *stream) {
     MassArgs g{conn, X, geo, U, P, gradP, dnode, snode, nlev, c1, Uo1, mo1, c2, Uo2, mo2, rho,
-               mdot, imbalance, adv};
+               mdot, imbalance, adv, rheology_of(0, 0.0, 0.0, 0.0, 2.0, 1.0), 0, 0, nullptr,
+               nullptr};
+    return dispatch<MassL>(kind, stored, g, n_colours, colour_offsets, as_stream(stream));
+}
+
+int zvfv_massflow_diag(int kind, int stored, const int32_t *conn, int n_colours,
+                       const int64_t *colour_offsets, const double *X, const double *geo,
+                       const double *U, const double *P, const double *gradP, const double *dnode,
+                       const double *snode, int nlev, double c1, const double *Uo1,
+                       const double *mo1, double c2, const double *Uo2, const double *mo2,
+                       double rho, int rheo, double mu0, double muinf, double lam, double ca,
+                       double cn, int transpose, int has_mut, const double *mut, double *mdot,
+                       double *imbalance, double *adv, double *vdiag, void *stream) {
+    if (!vdiag) {
+        set_error("massflow_diag: no viscous-diagonal output");
+        return BAD_ARGUMENT;
+    }
+    MassArgs g{conn, X, geo, U, P, gradP, dnode, snode, nlev, c1, Uo1, mo1, c2, Uo2, mo2, rho,
+               mdot, imbalance, adv, rheology_of(rheo, mu0, muinf, lam, ca, cn), transpose,
+               has_mut, mut, vdiag};
     return dispatch<MassL>(kind, stored, g, n_colours, colour_offsets, as_stream(stream));
 }
 

@@ -164,52 +164,56 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalise(const FinaliseArgs g) 
             g.rawb[i * 4 + r] = bi;
         }
         const bool fx = g.fixed[i * 4 + r];
+        const double uref = g.scal[0], pref = g.scal[1];
+        double s;
+        if (g.lscale[i] > 0.0 && r == 3) s = g.lscale[i] / uref;
+        else if (fx) s = r < 3 ? 1.0 / uref : 1.0 / pref;
+        else s = r < 3 ? 1.0 / (g.aP[i] * uref) : 1.0 / (g.rho * uref * pow(g.V[i], 2.0 / 3.0));
+        double ax = 0.0;
         if (fx) {
             for (long long p = p0; p < p1; ++p) {
                 double2 *row = reinterpret_cast<double2 *>(g.data + p * 16 + r * 4);
                 row[0] = make_double2(0.0, 0.0);
                 row[1] = make_double2(0.0, 0.0);
             }
-            g.data[pd * 16 + r * 5] = 1.0;
+            g.data[pd * 16 + r * 5] = s;          // the identity row, scaled
             bi = r < 3 ? g.vel[i * 3 + r] : g.pval[i];
-        } else if (g.eliminate) {
+            ax = g.x[i * 4 + r];
+        } else {
+            // one pass over the row: symmetric elimination of known columns, the row's product
+            // with the current state (for the residual report), and the scaled store - in the
+            // order of the separate passes they replace, so every sum is unchanged
+            const uchar4 *known4 = reinterpret_cast<const uchar4 *>(g.known);
             for (long long p = p0; p < p1; ++p) {
                 const long long j = g.indices[p];
-                for (int c = 0; c < 4; ++c)
-                    if (g.known[j * 4 + c]) {
-                        const double v = c < 3 ? g.vel[j * 3 + c] : g.pval[j];
-                        bi -= g.data[p * 16 + r * 4 + c] * v;
-                        g.data[p * 16 + r * 4 + c] = 0.0;
+                double2 *row = reinterpret_cast<double2 *>(g.data + p * 16 + r * 4);
+                double2 ra = row[0], rb = row[1];
+                if (g.eliminate) {
+                    const uchar4 kn = known4[j];
+                    if (kn.x | kn.y | kn.z | kn.w) {
+                        double a[4] = {ra.x, ra.y, rb.x, rb.y};
+                        const unsigned char k4[4] = {kn.x, kn.y, kn.z, kn.w};
+                        for (int c = 0; c < 4; ++c)
+                            if (k4[c]) {
+                                const double v = c < 3 ? g.vel[j * 3 + c] : g.pval[j];
+                                bi -= a[c] * v;
+                                a[c] = 0.0;
+                            }
+                        ra = make_double2(a[0], a[1]);
+                        rb = make_double2(a[2], a[3]);
                     }
+                }
+                const double2 xa = reinterpret_cast<const double2 *>(g.x)[j * 2];
+                const double2 xb = reinterpret_cast<const double2 *>(g.x)[j * 2 + 1];
+                ax += ra.x * xa.x + ra.y * xa.y + rb.x * xb.x + rb.y * xb.y;
+                row[0] = make_double2(ra.x * s, ra.y * s);
+                row[1] = make_double2(rb.x * s, rb.y * s);
             }
-        }
-        double ax = 0.0;
-        for (long long p = p0; p < p1; ++p) {
-            const long long j = g.indices[p];
-            const double2 *row = reinterpret_cast<const double2 *>(g.data + p * 16 + r * 4);
-            const double2 xa = reinterpret_cast<const double2 *>(g.x)[j * 2];
-            const double2 xb = reinterpret_cast<const double2 *>(g.x)[j * 2 + 1];
-            const double2 ra = row[0], rb = row[1];
-            ax += ra.x * xa.x + ra.y * xa.y + rb.x * xb.x + rb.y * xb.y;
-        }
-        if (!fx) {
             const double res = bi - ax;
             const double nrm = r < 3 ? g.aP[i] : g.rho * pow(g.V[i], 2.0 / 3.0);
             const double v = fabs(res) / nrm;
             sq = v * v;
             mx = v;
-        }
-        const double uref = g.scal[0], pref = g.scal[1];
-        double s;
-        if (g.lscale[i] > 0.0 && r == 3) s = g.lscale[i] / uref;
-        else if (fx) s = r < 3 ? 1.0 / uref : 1.0 / pref;
-        else s = r < 3 ? 1.0 / (g.aP[i] * uref) : 1.0 / (g.rho * uref * pow(g.V[i], 2.0 / 3.0));
-        for (long long p = p0; p < p1; ++p) {
-            double2 *row = reinterpret_cast<double2 *>(g.data + p * 16 + r * 4);
-            double2 ra = row[0], rb = row[1];
-            ra.x *= s; ra.y *= s; rb.x *= s; rb.y *= s;
-            row[0] = ra;
-            row[1] = rb;
         }
         g.b[i * 4 + r] = bi * s;
         g.rs_out[i * 4 + r] = s;

@@ -251,6 +251,8 @@ class Hierarchy {
         if (rebuild) {
             rebuild_requested = false;
             base_iterations = -1;
+            base_seen = 0;
+            ++rebuilds;
             drop_graphs();
             values.release();
             structure.release();
@@ -315,18 +317,24 @@ class Hierarchy {
         return OK;
     }
 
-    // Adaptive reuse (rebuild_every 0), the policy of the reference's AmgX binding
+    // Adaptive reuse (rebuild_every 0), after the policy of the reference's AmgX binding
     // (zvcfd/fv/linear.py:686-698, :837-841): later matrices keep the aggregates and only
     // re-sum the coarse operators, until a solve fails or needs more than rebuild_ratio times
-    // the iterations of the first solve after the last rebuild (and at least 2 more).
+    // (and at least 2 more than) the base iterations. The reference takes the first solve after
+    // a rebuild as the base; here it is the largest of the first BASE_SOLVES, because the
+    // coefficient loops of a time step alternate hard and easy solves and a base set by an
+    // easy one rebuilt the hierarchy on the next hard one, every step.
+    static constexpr int BASE_SOLVES = 3;
     bool rebuild_requested = false;
-    int base_iterations = -1;
+    int base_iterations = -1, base_seen = 0;
+    long long rebuilds = 0;
     void request_rebuild() { rebuild_requested = true; }
     void record_solve(int iterations, bool converged) {
         if (prm.rebuild_every > 0) return;
-        if (base_iterations < 0) {
-            base_iterations = iterations;
-            return;
+        if (base_seen < BASE_SOLVES) {
+            base_iterations = std::max(base_iterations, iterations);
+            ++base_seen;
+            if (converged) return;
         }
         const double limit = std::max(prm.rebuild_ratio * base_iterations, base_iterations + 2.0);
         if (!converged || iterations > limit) rebuild_requested = true;
@@ -440,7 +448,24 @@ class Hierarchy {
         const long long n = v.n;
         double *w;
         ZV_TRY(scratch.get(&w, v.nnz));
-        k_block_weight<<<grid_for(v.nnz, 256), 256, 0, st>>>(v.nnz, v.data, prm.strength, w); count_launch();
+        k_block_weight<<<grid_for(v.nnz, 256), 256, 0, st>>>(v.nnz, v.data, prm.strength == 1 ? 1 : 0,
+                                                             w); count_launch();
+        if (prm.strength == 2) {
+            // Convection makes the strongest coupling of a node point upstream, so that mutual
+            // strongest neighbours - the pairs of the matching - become rare and coarsening
+            // stalls (one level left). The mean of both directions keeps the pairs.
+            long long *tptr, *tperm;
+            int *trow;
+            double *ws;
+            ZV_TRY(scratch.get(&tptr, v.n + 1));
+            ZV_TRY(scratch.get(&trow, v.nnz));
+            ZV_TRY(scratch.get(&tperm, v.nnz));
+            ZV_TRY(scratch.get(&ws, v.nnz));
+            ZV_TRY(zvfv_bsr_transpose(v.n, v.nnz, (const int64_t *)v.indptr, v.indices,
+                                      (int64_t *)tptr, trow, (int64_t *)tperm, st));
+            k_symmetric_weight<<<grid_for(v.nnz, 256), 256, 0, st>>>(v.nnz, tperm, w, ws); count_launch();
+            w = ws;
+        }
         long long gn = n, gnnz = v.nnz;
         const long long *gptr = v.indptr;
         const int *gidx = v.indices;
@@ -1336,6 +1361,28 @@ int zvfv_solver_set_option(void *handle, const char *name, double value) {
         return BAD_ARGUMENT;
     }
     s->H.request_rebuild();                  // the next set-up builds with the new setting
+    return OK;
+}
+
+int zvfv_solver_get_option(void *handle, const char *name, double *value) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || !name || !value) {
+        set_error("solver_get_option: no handle, name or output");
+        return BAD_ARGUMENT;
+    }
+    const Params &p = s->H.prm;
+    const std::string opt(name);
+    if (opt == "autotune") *value = p.autotune;
+    else if (opt == "gs_levels") *value = p.gs_levels;
+    else if (opt == "jacobi_sweeps") *value = p.jacobi_sweeps;
+    else if (opt == "jacobi_omega") *value = p.jacobi_omega;
+    else if (opt == "rebuild_ratio") *value = p.rebuild_ratio;
+    else if (opt == "rebuilds") *value = (double)s->H.rebuilds;
+    else if (opt == "setups") *value = (double)s->H.setups;
+    else {
+        set_error("solver_get_option: unknown option %s", name);
+        return BAD_ARGUMENT;
+    }
     return OK;
 }
 

@@ -26,7 +26,7 @@ differences of full nonlinear solves.
 
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 from typing import Callable
 
 import numpy as np
@@ -80,7 +80,7 @@ def viscosity_mu0() -> Parameter:
         return float(s.fluid.viscosity.mu_0)
 
     def set_(s, v):
-        s.fluid.viscosity.mu_0 = float(v)
+        s.fluid.viscosity = replace(s.fluid.viscosity, mu_0=float(v))
         r = s.asm.rheo
         s.asm.rheo = (r[0], float(v)) + tuple(r[2:])
 
@@ -98,6 +98,18 @@ class FlowFractions:
         q = s.patch_flows()
         tot = sum(q[z] for z in self.zids)
         return torch.tensor([q[z] / tot for z in self.zids], dtype=torch.float64)
+
+
+class ZonePressures:
+    """Outputs: the area-mean pressure of each zone in ``zids``."""
+
+    def __init__(self, zids):
+        self.zids = list(zids)
+        self.names = [f"pressure[{z}]" for z in self.zids]
+
+    def __call__(self, s) -> torch.Tensor:
+        p = s.patch_pressures()
+        return torch.tensor([p[z] for z in self.zids], dtype=torch.float64)
 
 
 class MeanWallShear:
@@ -134,15 +146,19 @@ class SteadySensitivity:
         parameters: :class:`Parameter` list.
         outputs: callable ``solver -> (n_out,) tensor``.
         linear_rtol: tolerance of the linear solve inside each evaluation of ``Phi``.
-        eps: central-difference step in block-scaled state units.
+        eps: central-difference step in block-scaled state units. The error of a difference
+            quotient is about the linear solves' absolute accuracy (FGMRES stops at 1e-13 of
+            the right-hand side) times the condition of the system over ``eps``, plus
+            ``eps^2``: 1e-3 balances the two.
         rel_step: central-difference step of each parameter, relative to its value.
     """
 
-    def __init__(self, solver, parameters, outputs, *, linear_rtol: float = 1e-12,
-                 eps: float = 1e-5, rel_step: float = 1e-5, gmres_tol: float = 1e-9,
-                 restart: int = 40, maxiter: int = 200):
+    def __init__(self, solver, parameters, outputs, *, linear_rtol: float = 1e-10,
+                 eps: float = 1e-3, rel_step: float = 1e-4, gmres_tol: float = 1e-8,
+                 restart: int = 40, maxiter: int = 200, linear_maxiter: int = 1000):
         self.s, self.params, self.outputs = solver, list(parameters), outputs
         self.linear_rtol, self.eps, self.rel_step = linear_rtol, eps, rel_step
+        self.linear_maxiter = linear_maxiter
         self.gmres_tol, self.restart, self.maxiter = gmres_tol, restart, maxiter
         self.kinds = list(solver.mdot)
         self.z0 = self.state()
@@ -182,11 +198,22 @@ class SteadySensitivity:
         s = self.s
         self.set_state(z)
         keep = s.linear_rtol
+        keep_its = getattr(s.linear, "maxiter", None)
         s.linear_rtol = self.linear_rtol
+        if keep_its is not None:
+            s.linear.maxiter = self.linear_maxiter
         try:
-            s.iterate()
+            rec = s.iterate()
         finally:
             s.linear_rtol = keep
+            if keep_its is not None:
+                s.linear.maxiter = keep_its
+        # near the fixed point the initial residual is already small, and FGMRES stops at its
+        # round-off floor (1e-13 of the right-hand side) before a relative 1e-10; a solve that
+        # did not get within 1e-6 would put its error into every difference quotient
+        if rec["linear_residual"] > 1e-6:
+            raise RuntimeError(f"tight linear solve not converged ({rec['linear_residual']:.1e} "
+                               f"after {rec['linear_iterations']} iterations)")
         return self.state()
 
     def _with_param(self, p: Parameter, value: float, fn):
@@ -309,4 +336,4 @@ def steady_outputs(theta, solver, parameters, outputs, *, tol=1e-10, max_iterati
 
 
 __all__ = ["Parameter", "inlet_flow", "lumped", "viscosity_mu0", "FlowFractions",
-           "MeanWallShear", "Outputs", "SteadySensitivity", "SteadyOutputs", "steady_outputs"]
+           "ZonePressures", "MeanWallShear", "Outputs", "SteadySensitivity", "SteadyOutputs", "steady_outputs"]
