@@ -3,8 +3,8 @@
 Three small vessels of different kinds and sizes (a straight tet pipe, a curved hex/prism
 tube, a tet Y-bifurcation), each with its own inlet flow and RCR outlets, solved together as
 one block-diagonal system with the FP32 hierarchy and the lanes autotuner, reach each
-instance's own FP64 solution (solved alone) to 1e-7, and every instance's outflows balance
-its inflow.
+instance's own FP64 solution (solved alone; both to relative changes below 1e-9) to 1e-7,
+and every instance's outflows balance its inflow.
 """
 
 import numpy as np
@@ -46,11 +46,11 @@ def test_ensemble_matches_instances_solved_alone():
 
     cases = _cases()
     fl = Fluid(1060.0, 3.5e-3)
-    alone = solve_sequentially(cases, fl, tol=1e-10, max_iterations=600, advection=1.0)
+    alone = solve_sequentially(cases, fl, tol=1e-9, max_iterations=800, advection=1.0)
     assert all(r["converged"] for r in alone["instances"])
     ens = B200Ensemble(cases, fl, advection=1.0, linear="b200-mixed",
                        linear_options={"autotune": True})
-    rep = ens.solve(tol=1e-10, max_iterations=600)
+    rep = ens.solve(tol=1e-9, max_iterations=800)
     assert rep["converged"], rep["history"][-1]
     for i, r in enumerate(alone["instances"]):
         f = ens.fields(i)
