@@ -83,3 +83,41 @@ def test_oracle_wall_shear_matches_reference(name):
     tau = wall_shear(m, wall, g["U"], mu=fl.mu, viscosity=fl.viscosity)
     ref = load("wall_shear")[f"{name}_tau"]
     np.testing.assert_allclose(tau, ref, atol=1e-12 * np.abs(ref).max())
+
+
+def test_symmetrised_strength_keeps_pairwise_coarsening_under_convection():
+    """On a 12^3 lattice with one strong upstream coupling per node (a convective 4x4 block
+    system), the one-sided block-norm strength of the ACM's matching points every node at its
+    upstream neighbour, mutual pairs become rare and two passes leave 55 % of the rows; the
+    strength averaged over both directions of each coupling keeps the matching near 4:1."""
+    from oracle.linear import aggregate, transpose_positions
+
+    rng = np.random.default_rng(0)
+    nx = 12
+    n = nx ** 3
+    idx = np.arange(n).reshape(nx, nx, nx)
+    rows, cols, vals = [], [], []
+    for d in [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]:
+        sl = tuple(slice(max(0, -k), nx - max(0, k)) for k in d)
+        sh = tuple(slice(max(0, k), nx - max(0, -k)) for k in d)
+        a, b = idx[sl].ravel(), idx[sh].ravel()
+        if d == (0, 0, 0):
+            v = np.full(len(a), 10.0)
+        elif d == (-1, 0, 0):
+            v = -(5.0 + 0.1 * rng.random(len(a)))
+        else:
+            v = -(0.5 + 0.1 * rng.random(len(a)))
+        rows.append(a), cols.append(b), vals.append(v)
+    rows, cols, vals = (np.concatenate(x) for x in (rows, cols, vals))
+    o = np.lexsort((cols, rows))
+    rows, cols, vals = rows[o], cols[o], vals[o]
+    ip = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(rows, minlength=n), out=ip[1:])
+    pos = transpose_positions(ip, cols)
+    np.testing.assert_array_equal(rows[pos], cols)
+    np.testing.assert_array_equal(cols[pos], rows)
+    data = vals[:, None, None] * np.eye(4)[None]
+    _, one_sided = aggregate(ip, cols, data, 2, 0)
+    _, symmetric = aggregate(ip, cols, data, 2, 2)
+    assert one_sided > 0.5 * n
+    assert symmetric < 0.25 * n
