@@ -304,16 +304,21 @@ def ensemble_workload(args):
     from zvcfd_b200.ensemble import B200Ensemble, solve_sequentially, synthetic_ensemble
     from zvcfd_b200.fluid import Fluid
 
+    def log(msg):
+        print(msg, file=sys.stderr, flush=True)
+
     t0 = time.perf_counter()
     cases = synthetic_ensemble(count=args.instances, high=args.max_nodes, seed=0)
     gen = time.perf_counter() - t0
+    log(f"{len(cases)} meshes generated in {gen:.1f} s")
     fl = Fluid(1060.0, 3.5e-3)
     torch.cuda.synchronize()
-    seq = solve_sequentially(cases, fl, tol=1e-8, max_iterations=400, linear="b200")
+    seq = solve_sequentially(cases, fl, tol=1e-8, max_iterations=400, linear="b200", log=log)
     torch.cuda.synchronize()
     t = time.perf_counter()
     ens = B200Ensemble(cases, fl, linear="b200-mixed", linear_options={"autotune": True})
-    rep = ens.solve(tol=1e-8, max_iterations=400)
+    log(f"ensemble set up in {time.perf_counter() - t:.1f} s")
+    rep = ens.solve(tol=1e-8, max_iterations=400, log=log)
     torch.cuda.synchronize()
     t_ens = time.perf_counter() - t
     err = []
