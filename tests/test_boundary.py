@@ -66,3 +66,31 @@ def test_union_of_meshes_offsets_nodes_elements_and_zones():
             f, g = mesh.zones[z].faces, m.zones[u].faces
             np.testing.assert_array_equal(g, np.where(f >= 0, f + off[i], -1))
             assert m.zones[u].name.startswith(mesh.zones[z].name)
+
+
+def test_time_dependent_boundary_data_refresh_consistently():
+    """What a time step re-uploads (outlet pressure forces, known zone flows) equals the full
+    arrays of the same time, for a pulsatile inlet and a time-dependent outlet pressure."""
+    from zvcfd_b200.boundary import Boundary
+
+    g = load("pipe_reference_tube")
+    m = mesh_of(g)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    R = float(g["radius"])
+
+    def shape(x):
+        return np.clip(1 - (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2, 0, None)
+
+    bcs = {z["inlet"]: {"kind": "velocity", "flow_rate": lambda t: 0.3 + 0.1 * np.sin(t),
+                        "profile": shape},
+           z["outlet"]: {"kind": "pressure", "value": lambda x, t: 2.0 + np.cos(t) + 0 * x[:, 0]},
+           z["wall"]: {"kind": "wall"}}
+    b = Boundary(m, bcs, 1.0)
+    for t in (0.0, 0.7, 1.9):
+        b.update(t)
+        force = b.outlet_arrays()[0]
+        np.testing.assert_array_equal(b.outlet_force(), force)
+        assert np.abs(force).max() > 0
+        zids, W, c = b.flow_weights()
+        np.testing.assert_array_equal(b.flow_constants(zids), c)
+        assert abs(c[zids.index(z["inlet"])] + (0.3 + 0.1 * np.sin(t))) < 1e-12
