@@ -34,7 +34,8 @@ enum {
 
 const char *zvfv_last_error(void);
 int zvfv_version(void);
-/* kernels this library has launched since the process started */
+/* kernels this library has launched since the process started (a replayed V-cycle graph
+ * counts every kernel node it runs; its capture counts none) */
 int64_t zvfv_launch_count(void);
 /* doubles per stored geometry record of an element type (zvcfd/fv/fast.py:150-152) */
 int zvfv_record_doubles(int kind);

@@ -52,6 +52,9 @@ inline unsigned grid_for(long long work, int per_block) {
 
 // Every kernel launch of the library counts itself here (zvfv_launch_count reads the total).
 void count_launch();
+// A replayed CUDA graph counts its kernels (recorded while it was captured, when nothing ran).
+void count_launches(long long k);
+long long launches_so_far();
 
 // Number of SMs of the current device (cached per process; one device per process).
 int sm_count();

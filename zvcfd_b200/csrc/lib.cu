@@ -12,6 +12,8 @@ static thread_local char g_error[512] = "";
 static std::atomic<long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_error(const char *fmt, ...) {
     va_list ap;
