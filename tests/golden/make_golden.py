@@ -230,7 +230,39 @@ def wall_case() -> dict:
     return out
 
 
+def lumped_case() -> dict:
+    """The reference's RCR model (``zvcfd/lumped.py:181-218``): steady coefficients, and the
+    step coefficients and committed pressures of 40 steps under a pulsatile outflow, for the
+    trapezoidal and backward-Euler steppings, with a constant and a tabulated venous pressure."""
+    from zvcfd.lumped import RCR as RefRCR
+
+    out = {}
+    params = [(1e8, 1e-9, 1e9, 0.0), (2.0, 0.1, 5.0, 1.0), (0.5e8, 2e-9, 0.8e9, [(0.0, 100.0),
+                                                                            (0.4, 300.0),
+                                                                            (0.8, 100.0)])]
+    for i, (rp, c, rd, pv) in enumerate(params):
+        for method in ("trapezoidal", "euler"):
+            m = RefRCR(rp=rp, c=c, rd=rd, pv=pv, method=method)
+            a, r = m.steady_coefficients(0.0)
+            m.initialise(1e-6 if rp > 10 else 0.3, 0.0)
+            rows = []
+            dt = 0.013
+            for k in range(1, 41):
+                t = k * dt
+                q = (1e-6 if rp > 10 else 0.3) * (1.0 + 0.5 * np.sin(2 * np.pi * t / 0.8))
+                ca, cr = m.coefficients(t, dt)
+                p = m.advance(q, t, dt)
+                rows.append((t, q, ca, cr, p))
+            out[f"rcr{i}_{method}_steady"] = np.array([a, r])
+            out[f"rcr{i}_{method}_steps"] = np.array(rows)
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["lumped"]:
+        np.savez_compressed(HERE / "lumped.npz", **lumped_case())
+        print("wrote lumped")
+        return
     if sys.argv[1:] == ["wall"]:
         np.savez_compressed(HERE / "wall_shear.npz", **wall_case())
         print("wrote wall_shear")
@@ -257,6 +289,8 @@ def main():
     print("wrote transient_pipe")
     np.savez_compressed(HERE / "wall_shear.npz", **wall_case())
     print("wrote wall_shear")
+    np.savez_compressed(HERE / "lumped.npz", **lumped_case())
+    print("wrote lumped")
 
 
 if __name__ == "__main__":
