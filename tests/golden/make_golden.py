@@ -255,6 +255,17 @@ def lumped_case() -> dict:
                 rows.append((t, q, ca, cr, p))
             out[f"rcr{i}_{method}_steady"] = np.array([a, r])
             out[f"rcr{i}_{method}_steps"] = np.array(rows)
+    # the variable-step BDF coefficients and the Carreau-Yasuda law of the same module family
+    from zvcfd.fv.reference import bdf_coefficients
+    from zvcfd.rheology import CarreauYasuda as RefCY
+
+    cases = [("bdf1", 1e-3, None, 1), ("bdf2", 1e-3, None, 1), ("bdf2", 1e-3, 1e-3, 2),
+             ("bdf2", 2e-3, 1e-3, 2), ("bdf2", 0.5e-3, 1.5e-3, 2)]
+    out["bdf"] = np.array([bdf_coefficients(*c) for c in cases])
+    gamma = np.concatenate([[0.0], np.logspace(-3, 4, 29)])
+    out["cy_gamma"] = gamma
+    out["cy_blood"] = RefCY()(gamma)
+    out["cy_other"] = RefCY(mu_0=0.1, mu_inf=0.004, lam=1.5, a=1.7, n=0.4)(gamma)
     return out
 
 
