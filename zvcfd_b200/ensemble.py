@@ -54,11 +54,118 @@ def union(meshes: list) -> tuple:
     return Mesh(nodes, elements, zones), offsets, ids
 
 
+def segmented_fgmres(apply_A, apply_M, b, x0, seg, nseg: int, rtol: float, *, restart: int = 30,
+                     maxiter: int = 200):
+    """Right-preconditioned FGMRES with one Krylov recurrence per segment of a block-diagonal
+    system: every inner product, norm, Hessenberg column, Givens rotation and step length is
+    taken per segment (``seg``: the segment of each row), while the operator and the
+    preconditioner are applied to all segments at once. Each segment stops by its own
+    criterion, a reduction ``rtol`` of its initial residual (with the reference's round-off
+    floor of ``1e-13`` of its right-hand side); the iteration ends when all have.
+    Returns ``(x, iterations, largest relative residual, all converged)``."""
+    dt = b.dtype
+
+    def sdot(a, c):
+        return torch.zeros(nseg, dtype=dt, device=b.device).index_add_(0, seg, a * c)
+
+    x = x0.clone()
+    r = b - apply_A(x)
+    beta0 = torch.sqrt(sdot(r, r))
+    target = torch.maximum(rtol * beta0, 1e-13 * torch.sqrt(sdot(b, b)))
+    beta = beta0.clone()
+    its = 0
+    while its < maxiter and bool((beta > target).any()):
+        m = restart
+        H = torch.zeros((nseg, m + 1, m), dtype=dt, device=b.device)
+        cs = torch.zeros((nseg, m), dtype=dt, device=b.device)
+        sn = torch.zeros_like(cs)
+        g = torch.zeros((nseg, m + 1), dtype=dt, device=b.device)
+        g[:, 0] = beta
+        V = [r * torch.where(beta > 0, 1.0 / beta, torch.zeros_like(beta))[seg]]
+        Z = []
+        k_used = 0
+        for k in range(m):
+            Z.append(apply_M(V[k]))
+            w = apply_A(Z[k])
+            for _ in range(2):                                   # classical Gram-Schmidt, twice
+                h = torch.stack([sdot(V[j], w) for j in range(k + 1)])      # (k+1, nseg)
+                for j in range(k + 1):
+                    w = w - h[j][seg] * V[j]
+                H[:, :k + 1, k] += h.T
+            hn = torch.sqrt(sdot(w, w))
+            H[:, k + 1, k] = hn
+            V.append(w * torch.where(hn > 0, 1.0 / hn, torch.zeros_like(hn))[seg])
+            for j in range(k):                                   # earlier rotations
+                t = cs[:, j] * H[:, j, k] + sn[:, j] * H[:, j + 1, k]
+                H[:, j + 1, k] = -sn[:, j] * H[:, j, k] + cs[:, j] * H[:, j + 1, k]
+                H[:, j, k] = t
+            den = torch.hypot(H[:, k, k], H[:, k + 1, k])
+            ok = den > 0
+            cs[:, k] = torch.where(ok, H[:, k, k] / torch.where(ok, den, 1.0), 1.0)
+            sn[:, k] = torch.where(ok, H[:, k + 1, k] / torch.where(ok, den, 1.0), 0.0)
+            H[:, k, k] = den
+            H[:, k + 1, k] = 0.0
+            g[:, k + 1] = -sn[:, k] * g[:, k]
+            g[:, k] = cs[:, k] * g[:, k]
+            its += 1
+            k_used = k + 1
+            if bool((g[:, k + 1].abs() <= target).all()) or its >= maxiter:
+                break
+        R = H[:, :k_used, :k_used].clone()
+        rhs = g[:, :k_used].clone()
+        zero = R.diagonal(dim1=1, dim2=2) == 0                  # segments with nothing to solve
+        R.diagonal(dim1=1, dim2=2)[zero] = 1.0
+        rhs[zero] = 0.0
+        y = torch.linalg.solve_triangular(R, rhs[..., None], upper=True)[..., 0]
+        for j in range(k_used):
+            x = x + y[:, j][seg] * Z[j]
+        r = b - apply_A(x)
+        beta = torch.sqrt(sdot(r, r))
+    rel = beta / torch.where(beta0 > 0, beta0, torch.ones_like(beta0))
+    return x, its, float(rel.max()), bool((beta <= 1.01 * target).all())
+
+
+class SegmentedKrylov:
+    """A linear back end for the ensemble's union system: the AMG hierarchy of ``amg`` (built
+    on the union: block-diagonal, since its aggregates never cross instances) preconditions
+    :func:`segmented_fgmres` with one Krylov recurrence per instance (``krylov="segmented"``).
+
+    Experimental: the recurrences run in Python over torch tensors (tens of small launches and
+    a host read-back per Krylov step), and its one GPU run, the three-vessel ensemble test,
+    exceeded its 200 s limit; the algorithm itself is checked on the CPU. It is the shape of
+    the per-instance recurrences the union solve needs, to be moved into the device FGMRES."""
+
+    name = "b200-segmented"
+
+    def __init__(self, offsets, amg, *, restart: int = 30, maxiter: int = 200):
+        self.amg, self.restart, self.maxiter = amg, restart, maxiter
+        counts = torch.as_tensor(np.diff(offsets) * 4, device="cuda")
+        self.seg = torch.repeat_interleave(torch.arange(len(counts), device="cuda"), counts)
+        self.nseg = len(counts)
+        self.rtol = amg.rtol
+
+    def solve(self, A, b, x0=None, rtol=None):
+        from zvcfd_b200.linear import SolveInfo
+
+        ts = self.amg.setup(A)
+        t = time.time()
+        b = b.reshape(-1).contiguous()
+        x0 = torch.zeros_like(b) if x0 is None else x0.reshape(-1).contiguous()
+        x, its, res, ok = segmented_fgmres(A.matvec, self.amg.vcycle, b, x0, self.seg, self.nseg,
+                                           self.rtol if rtol is None else rtol,
+                                           restart=self.restart, maxiter=self.maxiter)
+        torch.cuda.synchronize()
+        return x, SolveInfo(its, res, time.time() - t, ts, ok)
+
+    def close(self):
+        self.amg.close()
+
+
 class B200Ensemble:
     """Independent steady problems ``cases = [(mesh, bcs), ...]`` of one fluid, solved together
     (see the module docstring). ``solver_options`` go to :class:`B200Solver`."""
 
-    def __init__(self, cases: list, fluid, **solver_options):
+    def __init__(self, cases: list, fluid, *, krylov: str = "union", **solver_options):
         meshes = [m for m, _ in cases]
         self.mesh, self.offsets, self.zone_ids = union(meshes)
         bcs = {}
@@ -66,6 +173,17 @@ class B200Ensemble:
             for z, spec in b.items():
                 bcs[self.zone_ids[i][z]] = spec
         self.n = len(cases)
+        if krylov == "segmented":
+            from zvcfd_b200.linear import B200AMG
+
+            lin = solver_options.pop("linear", "b200")
+            opts = dict(solver_options.pop("linear_options", None) or {})
+            rtol = solver_options.get("linear_rtol", 0.1)
+            amg = B200AMG(rtol=rtol, precision="mixed" if lin == "b200-mixed" else "double",
+                          **opts)
+            solver_options["linear"] = SegmentedKrylov(self.offsets, amg)
+        elif krylov != "union":
+            raise ValueError(f"krylov {krylov!r}: segmented or union")
         self.solver = B200Solver(self.mesh, fluid, bcs, **solver_options)
         self._len = torch.as_tensor(np.diff(self.offsets), device="cuda")
 
@@ -196,4 +314,5 @@ def synthetic_ensemble(count: int = 12, low: int = 50_000, high: int = 1_200_000
     return cases
 
 
-__all__ = ["union", "B200Ensemble", "solve_sequentially", "vessel", "synthetic_ensemble"]
+__all__ = ["union", "segmented_fgmres", "SegmentedKrylov", "B200Ensemble", "solve_sequentially",
+           "vessel", "synthetic_ensemble"]
