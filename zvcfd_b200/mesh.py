@@ -94,10 +94,22 @@ class Mesh:
                 faces.append(loc)
                 k = np.sort(loc, axis=1)
                 keys.append(k)
-        keys = np.concatenate(keys)
+        keys = np.concatenate(keys) + 1                 # -1 padding -> 0
         faces = np.concatenate(faces)
-        _, inv, cnt = np.unique(keys, axis=0, return_inverse=True, return_counts=True)
-        return faces[cnt[inv.reshape(-1)] == 1]
+        # two int64 keys per face (pairs of sorted node ids, each pair < (N + 1)^2) sorted
+        # together: a face is shared when its neighbour in that order has the same pair
+        base = np.int64(self.n_nodes + 1)
+        hi = keys[:, 0] * base + keys[:, 1]
+        lo = keys[:, 2] * base + keys[:, 3]
+        order = np.lexsort((lo, hi))
+        h, l_ = hi[order], lo[order]
+        same = (h[1:] == h[:-1]) & (l_[1:] == l_[:-1])
+        shared = np.zeros(len(order), bool)
+        shared[1:] |= same
+        shared[:-1] |= same
+        single = np.empty(len(order), bool)
+        single[order] = ~shared
+        return faces[single]
 
 
 # ---------------------------------------------------------------- splitting
