@@ -1,7 +1,7 @@
 """Adapters for the reference's own objects: CuPy arrays in and out, zero-copy.
 
-``ReferenceLinear`` is what ``zvcfd.fv.linear.make("b200")`` returns once bound
-(INTEGRATION.md): it takes the reference's ``BlockMatrix`` (``zvcfd/fv/linear.py:75-135``:
+``ReferenceLinear`` is what ``zvcfd.fv.linear.make("b200")`` returns once the reference's
+``make`` is given a ``"b200"`` branch: it takes the reference's ``BlockMatrix`` (``zvcfd/fv/linear.py:75-135``:
 CuPy ``indptr``/``indices``/``data`` and the ``lowrank`` list) and CuPy vectors, views them as
 torch tensors through ``__cuda_array_interface__`` (no copy), solves with
 :class:`~zvcfd_b200.linear.B200AMG`, and hands back a CuPy view of the solution and the
