@@ -116,3 +116,15 @@ def transient_bcs(g: dict, m):
 
     return {z["inlet"]: {"kind": "velocity", "value": prof},
             z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+
+
+def backflow_bcs(m, beta: float) -> dict:
+    """The backflow box's conditions (``tests/test_fv_boundaries.py:182-207`` of the reference):
+    walls, a uniform inflow at xmin, and at xmax a pressure ``1.5 cos(pi y)`` that pulls fluid
+    back in over part of the outlet, stabilised by ``beta``."""
+    z = {zz.name: k for k, zz in m.zones.items()}
+    bcs = {k: {"kind": "wall"} for k in m.zones}
+    bcs[z["xmin"]] = {"kind": "velocity", "value": (1.0, 0.0, 0.0)}
+    bcs[z["xmax"]] = {"kind": "pressure", "value": lambda x: 1.5 * np.cos(np.pi * x[:, 1]),
+                      "backflow_stabilisation": beta}
+    return bcs

@@ -230,6 +230,25 @@ def wall_case() -> dict:
     return out
 
 
+def backflow_case() -> dict:
+    """The reference's backflow box (``tests/test_fv_boundaries.py:182-207``): a warped tet
+    channel with a cosine outlet pressure that drives backflow, solved by the reference's CPU
+    solver with backflow stabilisation 0.5, and the same without stabilisation."""
+    m = box((6, 4, 3), (1.5, 1.0, 0.6), kind="tet", warp=0.03)
+    z = {b.name: k for k, b in m.zones.items()}
+    out = {}
+    for tag, beta in (("stab", 0.5), ("plain", 0.0)):
+        bcs = {k: {"kind": "wall"} for k in m.zones}
+        bcs[z["xmin"]] = {"kind": "velocity", "value": (1.0, 0.0, 0.0)}
+        bcs[z["xmax"]] = {"kind": "pressure", "value": lambda x: 1.5 * np.cos(np.pi * x[:, 1]),
+                          "backflow_stabilisation": beta}
+        s = ReferenceSolver(m, Fluid(1.0, 0.05), bcs, advection=1.0)
+        rep = s.solve(max_iterations=200, tol=1e-12)
+        assert rep.converged
+        out[f"U_{tag}"], out[f"P_{tag}"] = s.U.copy(), s.P.copy()
+    return dict(mesh_arrays(m), **out, rho=1.0, mu=0.05)
+
+
 def lumped_case() -> dict:
     """The reference's RCR model (``zvcfd/lumped.py:181-218``): steady coefficients, and the
     step coefficients and committed pressures of 40 steps under a pulsatile outflow, for the
@@ -270,6 +289,10 @@ def lumped_case() -> dict:
 
 
 def main():
+    if sys.argv[1:] == ["backflow"]:
+        np.savez_compressed(HERE / "backflow_box.npz", **backflow_case())
+        print("wrote backflow_box")
+        return
     if sys.argv[1:] == ["lumped"]:
         np.savez_compressed(HERE / "lumped.npz", **lumped_case())
         print("wrote lumped")
@@ -302,6 +325,8 @@ def main():
     print("wrote wall_shear")
     np.savez_compressed(HERE / "lumped.npz", **lumped_case())
     print("wrote lumped")
+    np.savez_compressed(HERE / "backflow_box.npz", **backflow_case())
+    print("wrote backflow_box")
 
 
 if __name__ == "__main__":

@@ -33,6 +33,46 @@ def test_boundary_arrays_match_oracle(name):
     assert len(zids) == len(m.zones)
 
 
+def test_backflow_stabilisation_weights_match_oracle():
+    """On the reference's backflow box the device path's outlet weights give, for the converged
+    mass flows of the oracle, the oracle's outflow momentum coefficient
+    ``m_b + beta max(-m_b, 0)`` shared by area, and the outlet force ``p S``."""
+    from fixtures import backflow_bcs
+    from zvcfd_b200.boundary import Boundary
+
+    g = load("backflow_box")
+    m = mesh_of(g)
+    bcs = backflow_bcs(m, 0.5)
+    o = OracleSolver(m, fluid_of(g), bcs, advection=1.0)
+    o.solve(max_iterations=200, tol=1e-12)
+    b = Boundary(m, bcs, float(g["rho"]))
+    force, a_out, w_cons, w_only, w_stab = b.outlet_arrays()
+    assert np.all(w_only == 0)
+    np.testing.assert_allclose(w_stab, 0.5 * w_cons, rtol=1e-15)
+    mb = o._mb
+    coef = w_cons * mb + w_stab * np.maximum(-mb, 0.0)
+    ref = np.zeros(o.N)
+    tot = o._pressure_area()
+    for zid, (f, S) in o.sub.items():
+        if bcs[zid]["kind"] != "pressure":
+            continue
+        ok = f >= 0
+        nodes = f[ok]
+        share = np.linalg.norm(S[ok], axis=1)
+        flow = mb[nodes] + 0.5 * np.maximum(-mb[nodes], 0.0)
+        ref += np.bincount(nodes, flow * share / tot[nodes], o.N)
+    np.testing.assert_allclose(coef, ref, atol=1e-14 * np.abs(ref).max())
+    pS = np.zeros((o.N, 3))
+    for zid, (f, S) in o.sub.items():
+        if bcs[zid]["kind"] == "pressure":
+            ok = f >= 0
+            flux = (o._outlet[zid][..., None] * S)[ok]
+            for k in range(3):
+                pS[:, k] += np.bincount(f[ok], flux[:, k], o.N)
+    assert np.abs(pS).max() > 0
+    np.testing.assert_allclose(force, pS, atol=1e-15 * np.abs(pS).max())
+
+
 def test_symmetry_and_pinned_pressure():
     from zvcfd_b200.boundary import Boundary
     from zvcfd_b200.mesh import box

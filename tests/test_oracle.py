@@ -71,6 +71,25 @@ def test_oracle_transient_matches_reference():
     np.testing.assert_allclose(s.P, g["P"], atol=1e-9 * np.ptp(g["P"]))
 
 
+@pytest.mark.parametrize("tag,beta", [("stab", 0.5), ("plain", 0.0)])
+def test_oracle_backflow_stabilisation_matches_reference(tag, beta):
+    """The reference's backflow box: part of the outlet carries inflow (m_b < 0), where the
+    stabilisation adds beta max(-m_b, 0) to the outflow momentum weight."""
+    from fixtures import backflow_bcs, fluid_of, mesh_of
+    from oracle.fv import OracleSolver
+
+    g = load("backflow_box")
+    m = mesh_of(g)
+    bcs = backflow_bcs(m, beta)
+    s = OracleSolver(m, fluid_of(g), bcs, advection=1.0)
+    rep = s.solve(max_iterations=200, tol=1e-12)
+    assert rep["converged"]
+    U, P = g[f"U_{tag}"], g[f"P_{tag}"]
+    np.testing.assert_allclose(s.U, U, atol=1e-9 * np.abs(U).max())
+    np.testing.assert_allclose(s.P, P, atol=1e-9 * np.ptp(P))
+    assert (s._mb[s.outlet] < 0).any() and (s._mb[s.outlet] > 0).any()
+
+
 @pytest.mark.parametrize("name", ["pipe_reference_tube", "curved_cy"])
 def test_oracle_wall_shear_matches_reference(name):
     from fixtures import fluid_of, mesh_of
