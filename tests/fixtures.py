@@ -128,3 +128,26 @@ def backflow_bcs(m, beta: float) -> dict:
     bcs[z["xmax"]] = {"kind": "pressure", "value": lambda x: 1.5 * np.cos(np.pi * x[:, 1]),
                       "backflow_stabilisation": beta}
     return bcs
+
+
+def forces_case(g: dict, tag: str):
+    """A zone-force golden case: its mesh and boundary conditions, rebuilt from the arrays."""
+    sub = {k[len(tag) + 1:]: v for k, v in g.items() if k.startswith(tag + "_")}
+    m = mesh_of(sub)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    if tag == "pipe":
+        R = 0.5
+
+        def prof(x):
+            r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+            return np.stack([0 * r2, 0 * r2, 2 * np.clip(1 - r2, 0, None)], 1)
+
+        bcs = {z["inlet"]: {"kind": "velocity", "value": prof},
+               z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    else:
+        bcs = {z["xmin"]: {"kind": "velocity", "value": [1.0, 0.0, 0.0]},
+               z["xmax"]: {"kind": "pressure", "value": 0.0},
+               z["ymax"]: {"kind": "pressure", "value": 0.0},
+               z["ymin"]: {"kind": "wall"}, z["zmin"]: {"kind": "symmetry"},
+               z["zmax"]: {"kind": "symmetry"}}
+    return m, bcs, sub

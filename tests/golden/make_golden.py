@@ -249,6 +249,88 @@ def backflow_case() -> dict:
     return dict(mesh_arrays(m), **out, rho=1.0, mu=0.05)
 
 
+def _host_gpusolver(s: ReferenceSolver):
+    """The reference's ``GPUSolver`` post-processing methods (``zone_forces``, ``wall_shear``,
+    ``zvcfd/fv/solver.py:1080-1245``) bound to the converged state of a CPU solve, with NumPy
+    standing in for CuPy (they only use array calls NumPy also has), so that their outputs can be
+    recorded here without a GPU."""
+    import types
+
+    from zvcfd.fv.solver import GPUSolver, RawRows
+
+    cp = types.ModuleType("cupy")
+    for k in dir(np):
+        if not k.startswith("_"):
+            setattr(cp, k, getattr(np, k))
+    cp.asnumpy = np.asarray
+    sys.modules.setdefault("cupy", cp)
+    g = object.__new__(GPUSolver)
+    g.cp, g.N, g._n_own = cp, s.N, s.N
+    g.mesh, g.fluid, g.bcs, g.stokes = s.mesh, s.fluid, s.bcs, s.stokes
+    g.sub, g.sub_flow, g.sub_vel = s.sub, s.sub_flow, s.sub_vel
+    g._outlet, g._special = s._outlet, {}
+    g.vel_fixed_comp = s.vel_fixed_comp
+    g.U, g.P = s.U.copy(), s.P.copy()
+    M, b = s._raw
+    indptr, indices = node_graph(s.mesh)
+    data = blocks_on_pattern(M, indptr, indices)
+    rows = np.repeat(np.arange(s.N), np.diff(indptr))
+    keep = np.flatnonzero(s.vel_fixed_comp.any(1)[rows])
+    g._raw = RawRows(keep, rows[keep], indices[keep].astype(np.int64), data[keep],
+                     b.reshape(-1, 4))
+    return g
+
+
+def forces_case() -> dict:
+    """Zone forces, zone flows and balances of two converged cases solved by the reference's
+    CPU solver: the mixed-element pipe of ``tests/test_fv_reference.py:152-162`` (walls, a
+    parabolic inlet, a pressure outlet; the case of ``tests/test_fv_solver_gpu.py:129-141``)
+    and the channel of ``tests/test_fv_boundaries.py:210-233`` (two pressure zones that share
+    an edge of nodes, a wall, two symmetry planes)."""
+    out = {}
+    R = 0.5
+    pipe = tube(R, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed", layers=1)
+    z = {zz.name: k for k, zz in pipe.zones.items()}
+
+    def prof(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+        return np.stack([0 * r2, 0 * r2, 2 * np.clip(1 - r2, 0, None)], 1)
+
+    pipe_bcs = {z["inlet"]: {"kind": "velocity", "value": prof},
+                z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    chan = box((10, 6, 1), (2.0, 1.0, 0.2), kind="hex")
+    z = {zz.name: k for k, zz in chan.zones.items()}
+    chan_bcs = {z["xmin"]: {"kind": "velocity", "value": [1.0, 0.0, 0.0]},
+                z["xmax"]: {"kind": "pressure", "value": 0.0},
+                z["ymax"]: {"kind": "pressure", "value": 0.0},
+                z["ymin"]: {"kind": "wall"}, z["zmin"]: {"kind": "symmetry"},
+                z["zmax"]: {"kind": "symmetry"}}
+    for tag, m, bcs, mu in (("pipe", pipe, pipe_bcs, 0.2), ("channel", chan, chan_bcs, 0.05)):
+        s = ReferenceSolver(m, Fluid(1.0, mu), bcs, advection=1.0)
+        rep = s.solve(max_iterations=300, tol=1e-13)
+        assert rep.converged
+        F, q, bal = s.zone_forces(), s.zone_flows(), s.balances()
+        zids = sorted(F)
+        for k, v in mesh_arrays(m).items():
+            out[f"{tag}_{k}"] = v
+        out.update({f"{tag}_U": s.U.copy(), f"{tag}_P": s.P.copy(), f"{tag}_mu": mu,
+                    f"{tag}_force_zones": np.array(zids, np.int64),
+                    f"{tag}_forces": np.array([F[k] for k in zids]),
+                    f"{tag}_flows": np.array([q[k] for k in zids]),
+                    f"{tag}_momentum_outflow": np.array(
+                        [s.zone_momentum_outflow()[k] for k in zids]),
+                    f"{tag}_mass": bal["mass"], f"{tag}_momentum": bal["momentum"],
+                    f"{tag}_identity": bal["identity"]})
+        h = _host_gpusolver(s)
+        Fg = h.zone_forces()
+        out[f"{tag}_gpusolver_forces"] = np.array([Fg[k] for k in zids])
+        nodes, tau = h.wall_shear("reaction")
+        out[f"{tag}_reaction_nodes"], out[f"{tag}_reaction_tau"] = nodes, tau
+        nodes, tau = h.wall_shear("gradient")
+        out[f"{tag}_gradient_nodes"], out[f"{tag}_gradient_tau"] = nodes, tau
+    return out
+
+
 def lumped_case() -> dict:
     """The reference's RCR model (``zvcfd/lumped.py:181-218``): steady coefficients, and the
     step coefficients and committed pressures of 40 steps under a pulsatile outflow, for the
@@ -289,6 +371,10 @@ def lumped_case() -> dict:
 
 
 def main():
+    if sys.argv[1:] == ["forces"]:
+        np.savez_compressed(HERE / "forces.npz", **forces_case())
+        print("wrote forces")
+        return
     if sys.argv[1:] == ["backflow"]:
         np.savez_compressed(HERE / "backflow_box.npz", **backflow_case())
         print("wrote backflow_box")
@@ -327,6 +413,8 @@ def main():
     print("wrote lumped")
     np.savez_compressed(HERE / "backflow_box.npz", **backflow_case())
     print("wrote backflow_box")
+    np.savez_compressed(HERE / "forces.npz", **forces_case())
+    print("wrote forces")
 
 
 if __name__ == "__main__":

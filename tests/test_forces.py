@@ -1,0 +1,121 @@
+"""Zone forces from consistent reactions: the oracle and the device path's host code against
+the reference's own forces (CPU)."""
+
+import numpy as np
+import pytest
+import torch
+
+from fixtures import forces_case, load
+from oracle.fv import OracleSolver
+from zvcfd_b200.fluid import Fluid
+
+
+def _solved(tag):
+    g = load("forces")
+    m, bcs, sub = forces_case(g, tag)
+    s = OracleSolver(m, Fluid(1.0, float(sub["mu"])), bcs, advection=1.0)
+    assert s.solve(max_iterations=300, tol=1e-13)["converged"]
+    return m, bcs, sub, s
+
+
+def _compact(s, keep):
+    """The oracle's raw rows in the device path's layout: kept rows' blocks contiguous."""
+    ip = s.indptr.astype(np.int64)
+    cnt = np.where(keep, ip[1:] - ip[:-1], 0)
+    rawoff = np.where(keep, np.cumsum(cnt) - cnt, -1)
+    data, b = s.raw
+    blocks = np.concatenate([data[ip[i]:ip[i + 1]] for i in np.flatnonzero(keep)])
+    rawb = np.where(keep[:, None], b, 0.0)
+    return (torch.as_tensor(ip), torch.as_tensor(s.indices.astype(np.int32)),
+            torch.as_tensor(rawoff), torch.as_tensor(blocks.reshape(-1)), torch.as_tensor(rawb))
+
+
+@pytest.mark.parametrize("tag", ["pipe", "channel"])
+def test_oracle_zone_forces_match_reference(tag):
+    """The reference's ``test_zone_forces_match_reference`` case (and the channel with two
+    pressure zones and symmetry planes): forces to 1e-12 of their scale, flows to 1e-12."""
+    _, _, sub, s = _solved(tag)
+    F, q = s.zone_forces(), s.zone_flows()
+    zids = [int(z) for z in sub["force_zones"]]
+    scale = np.abs(sub["forces"]).max()
+    np.testing.assert_allclose(np.array([F[z] for z in zids]), sub["forces"], atol=1e-12 * scale)
+    np.testing.assert_allclose(np.array([q[z] for z in zids]), sub["flows"],
+                               atol=1e-12 * np.abs(sub["flows"]).max())
+    # the momentum balance the forces close: sum of forces and momentum outflows
+    Mo = sub["momentum_outflow"]
+    assert np.abs((sub["forces"] + Mo).sum(0)).max() < 1e-12 * scale
+
+
+@pytest.mark.parametrize("tag", ["pipe", "channel"])
+def test_device_path_zone_forces_from_compact_raw_rows(tag):
+    """:class:`zvcfd_b200.forces.RawRows` over the compact kept-row layout the boundary pass
+    writes, and :func:`zvcfd_b200.forces.zone_forces` over the device path's boundary data,
+    give the reference's forces."""
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.forces import RawRows, zone_forces
+
+    m, bcs, sub, s = _solved(tag)
+    bc = Boundary(m, bcs, 1.0)
+    keep = bc.vel_fixed_comp.any(1)
+    raw = RawRows(*_compact(s, keep))
+    X = torch.as_tensor(np.concatenate([s.U, s.P[:, None]], 1))
+    r = raw.residual(X).numpy()
+    full = s.momentum_residual()
+    np.testing.assert_allclose(r[keep, :3], full[keep], atol=1e-13 * np.abs(full).max())
+    assert np.all(r[~keep] == 0)
+    F = zone_forces(bc, r, s.P)
+    zids = [int(z) for z in sub["force_zones"]]
+    scale = np.abs(sub["forces"]).max()
+    np.testing.assert_allclose(np.array([F[z] for z in zids]), sub["forces"], atol=1e-12 * scale)
+
+
+@pytest.mark.parametrize("tag", ["pipe", "channel"])
+def test_device_path_reaction_wall_shear_matches_reference(tag):
+    """``wall_shear(method="reaction")``: the reference device solver's own evaluation of the
+    converged state (recorded with NumPy in place of CuPy) against the device path's host code
+    over the compact kept rows; also its zone forces, which equal the CPU reference's."""
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.forces import RawRows, wall_shear_reaction
+
+    m, bcs, sub, s = _solved(tag)
+    np.testing.assert_allclose(sub["gpusolver_forces"], sub["forces"],
+                               atol=1e-13 * np.abs(sub["forces"]).max())
+    bc = Boundary(m, bcs, 1.0)
+    raw = RawRows(*_compact(s, bc.vel_fixed_comp.any(1)))
+    r = raw.residual(torch.as_tensor(np.concatenate([s.U, s.P[:, None]], 1))).numpy()
+    nodes, tau = wall_shear_reaction(bc, r, s.P)
+    np.testing.assert_array_equal(nodes, sub["reaction_nodes"])
+    ref = sub["reaction_tau"]
+    np.testing.assert_allclose(tau, ref, atol=1e-11 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("tag", ["pipe", "channel"])
+def test_oracle_gradient_wall_shear_matches_reference_device_solver(tag):
+    """``wall_shear()`` (the gradient method) of the reference device solver on the converged
+    state equals the oracle's wall-gradient evaluator at the same nodes."""
+    from oracle.wall import wall_shear
+
+    m, bcs, sub, s = _solved(tag)
+    walls = [z for z in m.zones if bcs[z]["kind"] == "wall"]
+    tau = wall_shear(m, walls, s.U, mu=float(sub["mu"]))
+    np.testing.assert_array_equal(sub["gradient_nodes"], sub["reaction_nodes"])
+    ref = sub["gradient_tau"]
+    np.testing.assert_allclose(tau[sub["gradient_nodes"]], ref, atol=1e-12 * np.abs(ref).max())
+
+
+def test_raw_rows_residual_on_a_random_state():
+    """At a random state the kept rows' residual equals the full system's, row by row."""
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.forces import RawRows
+
+    m, bcs, sub, s = _solved("channel")
+    keep = Boundary(m, bcs, 1.0).vel_fixed_comp.any(1)
+    rng = np.random.default_rng(3)
+    s.U, s.P = rng.standard_normal((s.N, 3)), rng.standard_normal(s.N)
+    raw = RawRows(*_compact(s, keep))
+    r = raw.residual(torch.as_tensor(np.concatenate([s.U, s.P[:, None]], 1))).numpy()
+    data, b = s.raw
+    full = (s.to_csr(data) @ np.concatenate([s.U, s.P[:, None]], 1).reshape(-1)
+            - b.reshape(-1)).reshape(-1, 4)
+    np.testing.assert_allclose(r[keep], full[keep], atol=1e-12 * np.abs(full).max())
+    assert raw.nraw == int(np.sum((s.indptr[1:] - s.indptr[:-1])[keep]))
