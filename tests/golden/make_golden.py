@@ -331,6 +331,24 @@ def forces_case() -> dict:
     return out
 
 
+def wss_case() -> dict:
+    """The reference's WSS time statistics (``zvcfd/fv/wss.py``) over a seeded series: 40 wall
+    nodes, 9 samples at uneven times; node 0 never sheared, node 1 reverses in time."""
+    from zvcfd.fv.wss import WallShearStats
+
+    rng = np.random.default_rng(11)
+    n, k = 40, 9
+    t = np.cumsum(rng.uniform(0.5e-3, 2e-3, k))
+    tau = rng.standard_normal((k, n, 3))
+    tau[:, 0] = 0.0
+    tau[:, 1] = np.sin(2 * np.pi * (t - t[0]) / (t[-1] - t[0]))[:, None] * np.array([1.0, 0.2, 0])
+    st = WallShearStats(n)
+    for ti, x in zip(t, tau):
+        st.add(ti, x)
+    r = st.results()
+    return {"t": t, "tau": tau, "tawss": r["tawss"], "osi": r["osi"], "rrt": r["rrt"]}
+
+
 def lumped_case() -> dict:
     """The reference's RCR model (``zvcfd/lumped.py:181-218``): steady coefficients, and the
     step coefficients and committed pressures of 40 steps under a pulsatile outflow, for the
@@ -371,6 +389,10 @@ def lumped_case() -> dict:
 
 
 def main():
+    if sys.argv[1:] == ["wss"]:
+        np.savez_compressed(HERE / "wss.npz", **wss_case())
+        print("wrote wss")
+        return
     if sys.argv[1:] == ["forces"]:
         np.savez_compressed(HERE / "forces.npz", **forces_case())
         print("wrote forces")
@@ -415,6 +437,8 @@ def main():
     print("wrote backflow_box")
     np.savez_compressed(HERE / "forces.npz", **forces_case())
     print("wrote forces")
+    np.savez_compressed(HERE / "wss.npz", **wss_case())
+    print("wrote wss")
 
 
 if __name__ == "__main__":
