@@ -103,6 +103,26 @@ def test_oracle_gradient_wall_shear_matches_reference_device_solver(tag):
     np.testing.assert_allclose(tau[sub["gradient_nodes"]], ref, atol=1e-12 * np.abs(ref).max())
 
 
+def test_zone_flows_split_a_shared_edge_by_area():
+    """The channel whose outflow and top pressure zones share an edge of nodes
+    (``tests/test_fv_boundaries.py:210-233`` of the reference): the device path's zone-flow
+    weights (``W m_b + c``, read back once per iteration) applied to the oracle's converged
+    boundary mass flows give the reference's zone flows, each shared node counted once."""
+    from zvcfd_b200.boundary import Boundary
+
+    m, bcs, sub, s = _solved("channel")
+    zids, W, c = Boundary(m, bcs, 1.0).flow_weights()
+    q = dict(zip(zids, W @ s._mb + c))
+    ref = dict(zip([int(z) for z in sub["force_zones"]], sub["flows"]))
+    assert sorted(q) == sorted(ref)
+    scale = sum(abs(v) for v in ref.values())
+    for z in ref:
+        assert abs(q[z] - ref[z]) < 1e-12 * scale
+    name = {zz.name: k for k, zz in m.zones.items()}
+    assert q[name["xmax"]] > 0 and q[name["ymax"]] > 0
+    assert abs(sum(q.values())) < 1e-12 * scale
+
+
 def test_raw_rows_residual_on_a_random_state():
     """At a random state the kept rows' residual equals the full system's, row by row."""
     from zvcfd_b200.boundary import Boundary
