@@ -4,7 +4,7 @@
 ``make`` is given a ``"b200"`` branch: it takes the reference's ``BlockMatrix`` (``zvcfd/fv/linear.py:75-135``:
 CuPy ``indptr``/``indices``/``data`` and the ``lowrank`` list) and CuPy vectors, views them as
 torch tensors through ``__cuda_array_interface__`` (no copy), solves with
-:class:`~zvcfd_b200.linear.B200AMG`, and hands back a CuPy view of the solution and the
+:class:`~zvcfd_b200.linear.B200AMG` (or the ``b200-auto`` ladder), and hands back a CuPy view of the solution and the
 reference's ``SolveInfo`` fields. ``ReferenceAssembler`` does the same for
 :class:`~zvcfd_b200.assembler.B200Assembler`'s ``FastAssembler`` interface.
 """
@@ -14,7 +14,7 @@ from __future__ import annotations
 import torch
 
 from zvcfd_b200.assembler import B200Assembler
-from zvcfd_b200.linear import B200AMG, BlockMatrix
+from zvcfd_b200.linear import BlockMatrix, make
 
 
 def as_torch(a):
@@ -53,10 +53,17 @@ class ReferenceLinear:
     """``solve(A, b, x0=None, rtol=None) -> (x, SolveInfo)`` over the reference's objects."""
 
     def __init__(self, name: str = "b200", **kw):
-        if name == "b200-mixed":
-            kw = {"precision": "mixed"} | kw
-        self.inner = B200AMG(**kw)
+        self.inner = make(name, **kw)
         self.name = name
+
+    @property
+    def active(self) -> str:
+        """The rung in use (``"b200-auto"``), as the reference's ``Auto.active``."""
+        return getattr(self.inner, "active", self.name)
+
+    @property
+    def switches(self) -> list:
+        return getattr(self.inner, "switches", [])
 
     def solve(self, A, b, x0=None, rtol=None):
         x, info = self.inner.solve(block_matrix(A), as_torch(b).reshape(-1),
