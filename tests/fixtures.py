@@ -151,3 +151,36 @@ def forces_case(g: dict, tag: str):
                z["ymin"]: {"kind": "wall"}, z["zmin"]: {"kind": "symmetry"},
                z["zmax"]: {"kind": "symmetry"}}
     return m, bcs, sub
+
+
+def tabulated(points: np.ndarray, values: np.ndarray):
+    """``f(x)`` that returns the tabulated value at each of the points ``x`` (each must be one
+    of ``points`` up to round-off): boundary data recorded where the reference evaluated it."""
+    from scipy.spatial import cKDTree
+
+    tree = cKDTree(points)
+    scale = float(np.abs(points).max())
+
+    def f(x):
+        d, i = tree.query(np.asarray(x, float))
+        if np.any(d > 1e-12 * scale):
+            raise KeyError("a point the table does not hold")
+        return values[i]
+
+    return f
+
+
+def gn_outlet_bcs(g: dict, m) -> dict:
+    """The manufactured Carreau-Yasuda outlet case's conditions, from its tables."""
+    z = {zz.name: k for k, zz in m.zones.items()}
+    u, p, J = (tabulated(g["points"], g[k]) for k in ("u", "p", "J"))
+    bcs = {k: {"kind": "velocity", "value": u} for k in m.zones}
+    bcs[z["xmax"]] = {"kind": "pressure", "value": p, "grad": J}
+    return bcs
+
+
+def gn_outlet_fluid(g: dict):
+    from zvcfd_b200.fluid import CarreauYasuda, Fluid
+
+    return Fluid(float(g["rho"]), float(g["mu"]),
+                 viscosity=CarreauYasuda(*[float(v) for v in g["cy"]]))

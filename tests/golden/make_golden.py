@@ -21,6 +21,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
+REFERENCE = "/root/reference"          # the reference's source tree (also on PYTHONPATH)
 sys.path.insert(0, str(HERE.parents[1]))
 
 from zvcfd.fv.geometry import topology  # noqa: E402  (the reference)
@@ -349,6 +350,44 @@ def wss_case() -> dict:
     return {"t": t, "tau": tau, "tawss": r["tawss"], "osi": r["osi"], "rrt": r["rrt"]}
 
 
+def gn_outlet_case() -> dict:
+    """The reference's Carreau-Yasuda manufactured outlet (``tests/test_fv_solver_gpu.py:76-101``):
+    a warped tet box with the manufactured velocity on every face but ``xmax``, a pressure
+    outlet there with the manufactured pressure and prescribed velocity gradient (traction),
+    the manufactured body force, the transpose term on; solved by the reference's CPU solver.
+    The manufactured fields are tabulated at the nodes and the outlet's sub-face points (where
+    the conditions are evaluated), so that the tests can rebuild the conditions without it."""
+    from zvcfd.fv.geometry import boundary_subface_weights
+    from zvcfd.rheology import CarreauYasuda as RefCY
+
+    sys.path.insert(0, str(Path(REFERENCE) / "benchmarks" / "validation"))
+    from exact import manufactured_gn
+
+    cy = RefCY(mu_0=0.5, mu_inf=0.05, lam=2.0)
+    m = box((4, 4, 4), kind="tet", warp=0.03)
+
+    def ex(x):
+        return manufactured_gn(x, cy.of_gamma_squared, shift=(0.2, 0.1, 0.3),
+                               mean=(1.5, 0.0, 0.0))
+
+    z = {b.name: k for k, b in m.zones.items()}
+    bcs = {k: {"kind": "velocity", "value": lambda x: ex(x)[0]} for k in m.zones}
+    bcs[z["xmax"]] = {"kind": "pressure", "value": lambda x: ex(x)[1],
+                      "grad": lambda x: ex(x)[3]}
+    s = ReferenceSolver(m, Fluid(1.0, 0.1, viscosity=lambda g: cy.of_gamma_squared(g * g)),
+                        bcs, source=lambda x: ex(x)[2], advection=1.0, transpose=True)
+    rep = s.solve(max_iterations=200, tol=1e-13)
+    assert rep.converged
+    f = m.zones[z["xmax"]].faces
+    ok = f >= 0
+    xs = np.einsum("fij,fjk->fik", boundary_subface_weights(f), m.nodes[np.where(ok, f, 0)])
+    pts = np.concatenate([m.nodes, xs[ok]])
+    u, p, src, J = ex(pts)
+    return dict(mesh_arrays(m), U=s.U.copy(), P=s.P.copy(), rho=1.0, mu=0.1,
+                cy=np.array([cy.mu_0, cy.mu_inf, cy.lam, cy.a, cy.n]), points=pts, u=u, p=p,
+                f=src, J=J, iterations=rep.iterations)
+
+
 def lumped_case() -> dict:
     """The reference's RCR model (``zvcfd/lumped.py:181-218``): steady coefficients, and the
     step coefficients and committed pressures of 40 steps under a pulsatile outflow, for the
@@ -389,6 +428,10 @@ def lumped_case() -> dict:
 
 
 def main():
+    if sys.argv[1:] == ["gn_outlet"]:
+        np.savez_compressed(HERE / "gn_outlet.npz", **gn_outlet_case())
+        print("wrote gn_outlet")
+        return
     if sys.argv[1:] == ["wss"]:
         np.savez_compressed(HERE / "wss.npz", **wss_case())
         print("wrote wss")
@@ -439,6 +482,8 @@ def main():
     print("wrote forces")
     np.savez_compressed(HERE / "wss.npz", **wss_case())
     print("wrote wss")
+    np.savez_compressed(HERE / "gn_outlet.npz", **gn_outlet_case())
+    print("wrote gn_outlet")
 
 
 if __name__ == "__main__":

@@ -73,6 +73,37 @@ def test_backflow_stabilisation_weights_match_oracle():
     np.testing.assert_allclose(force, pS, atol=1e-15 * np.abs(pS).max())
 
 
+@pytest.mark.parametrize("transpose", [True, False])
+def test_prescribed_outlet_gradient_traction_matches_oracle(transpose):
+    """A pressure zone with a prescribed velocity gradient: the device path's outlet force is
+    the oracle's ``p S - mu(grad) tau S`` (``tau = grad + grad^T`` with the transpose term),
+    and the zone takes no part in the lagged transpose traction."""
+    from fixtures import gn_outlet_bcs, gn_outlet_fluid, tabulated
+    from zvcfd_b200.boundary import Boundary
+
+    g = load("gn_outlet")
+    m = mesh_of(g)
+    bcs = gn_outlet_bcs(g, m)
+    fl = gn_outlet_fluid(g)
+    o = OracleSolver(m, fl, bcs, source=tabulated(g["points"], g["f"]), advection=1.0,
+                     transpose=transpose)
+    b = Boundary(m, bcs, fl.rho, mu=fl.mu, viscosity=fl.viscosity, transpose=transpose)
+    force, a_out, *_ = b.outlet_arrays()
+    data = np.zeros((len(o.indices), 4, 4))
+    rhs = np.zeros((o.N, 4))
+    o._mb = np.zeros(o.N)
+    o._outlet_terms(data, rhs, o.diagonal_positions(), np.zeros((o.N, 3, 3)))
+    ref = -rhs[:, :3]
+    assert np.abs(ref).max() > 0
+    np.testing.assert_allclose(force, ref, atol=1e-14 * np.abs(ref).max())
+    assert np.all(a_out == 0)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    bad = dict(bcs)
+    bad[z["xmax"]] = dict(bcs[z["xmax"]], lumped=object())
+    with pytest.raises(ValueError, match="grad"):
+        Boundary(m, bad, 1.0)
+
+
 def test_symmetry_and_pinned_pressure():
     from zvcfd_b200.boundary import Boundary
     from zvcfd_b200.mesh import box

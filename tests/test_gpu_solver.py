@@ -179,3 +179,23 @@ def test_zone_forces_and_wall_shear_match_reference(tag):
     np.testing.assert_allclose(tau, sub["gradient_tau"],
                                atol=1e-7 * np.abs(sub["gradient_tau"]).max())
     s.close()
+
+
+def test_manufactured_carreau_outlet_matches_reference():
+    """The reference's ``test_carreau_outlet_manufactured`` (``tests/test_fv_solver_gpu.py``
+    ``:76-101``): a body force, a pressure outlet with a prescribed velocity gradient
+    (traction), Carreau-Yasuda viscosity and the transpose term; velocity to 1e-8 of the
+    reference's solution, as the reference's own test asks."""
+    from fixtures import gn_outlet_bcs, gn_outlet_fluid, tabulated
+    from zvcfd_b200.solver import B200Solver
+
+    g = load("gn_outlet")
+    m = mesh_of(g)
+    s = B200Solver(m, gn_outlet_fluid(g), gn_outlet_bcs(g, m),
+                   source=tabulated(g["points"], g["f"]), advection=1.0, transpose=True)
+    rep = s.solve(max_iterations=800, tol=1e-11)
+    assert rep["converged"], rep["history"][-1]
+    f = s.fields()
+    np.testing.assert_allclose(f["U"], g["U"], atol=1e-8 * np.abs(g["U"]).max())
+    np.testing.assert_allclose(f["P"], g["P"], atol=1e-8 * np.ptp(g["P"]))
+    s.close()

@@ -90,6 +90,21 @@ def test_oracle_backflow_stabilisation_matches_reference(tag, beta):
     assert (s._mb[s.outlet] < 0).any() and (s._mb[s.outlet] > 0).any()
 
 
+def test_oracle_manufactured_carreau_outlet_matches_reference():
+    """The reference's Carreau-Yasuda manufactured outlet (``tests/test_fv_solver_gpu.py``
+    ``:76-101``): body force, prescribed outlet gradient (traction), transpose term."""
+    from fixtures import gn_outlet_bcs, gn_outlet_fluid, mesh_of, tabulated
+    from oracle.fv import OracleSolver
+
+    g = load("gn_outlet")
+    m = mesh_of(g)
+    s = OracleSolver(m, gn_outlet_fluid(g), gn_outlet_bcs(g, m),
+                     source=tabulated(g["points"], g["f"]), advection=1.0, transpose=True)
+    assert s.solve(max_iterations=300, tol=1e-13)["converged"]
+    np.testing.assert_allclose(s.U, g["U"], atol=1e-11 * np.abs(g["U"]).max())
+    np.testing.assert_allclose(s.P, g["P"], atol=1e-11 * np.ptp(g["P"]))
+
+
 @pytest.mark.parametrize("name", ["pipe_reference_tube", "curved_cy"])
 def test_oracle_wall_shear_matches_reference(name):
     from fixtures import fluid_of, mesh_of
