@@ -104,6 +104,20 @@ def test_prescribed_outlet_gradient_traction_matches_oracle(transpose):
         Boundary(m, bad, 1.0)
 
 
+@pytest.mark.parametrize("extra", [{"profile": "average"}, {"opening": True}])
+def test_unsupported_pressure_zones_are_refused(extra):
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.mesh import box
+
+    m = box((3, 2, 2), kind="hex")
+    z = {zz.name: k for k, zz in m.zones.items()}
+    bcs = {k: {"kind": "wall"} for k in m.zones}
+    bcs[z["xmin"]] = {"kind": "velocity", "value": (1.0, 0.0, 0.0)}
+    bcs[z["xmax"]] = {"kind": "pressure", "value": 0.0, **extra}
+    with pytest.raises(NotImplementedError):
+        Boundary(m, bcs, 1.0)
+
+
 def test_symmetry_and_pinned_pressure():
     from zvcfd_b200.boundary import Boundary
     from zvcfd_b200.mesh import box
