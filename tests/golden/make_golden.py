@@ -9,8 +9,14 @@ meshes (every element type) the reference's node volumes, nodal gradients,
 momentum diagonal, limiter, raw assembled block system, pattern and new mass
 flows on a seeded random state (the procedure of the reference's
 ``tests/test_fv_fast.py:98-159``), plus converged fields of three small pipes
-solved by the reference's CPU solver with lagged Rhie-Chow. Nothing at test or
-bench time reads the reference: the tests read these files.
+solved by the reference's CPU solver with lagged Rhie-Chow; a pulsatile BDF2
+pipe (``transient``); wall shear (``wall``); the 0-D RCR model, BDF
+coefficients and Carreau-Yasuda viscosity (``lumped``); the backflow box with
+and without stabilisation (``backflow``); zone forces, flows and both wall-shear
+methods of two converged cases (``forces``); WSS time statistics (``wss``);
+the manufactured Carreau-Yasuda outlet (``gn_outlet``). A single file is
+rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
+at test or bench time reads the reference: the tests read these files.
 """
 
 from __future__ import annotations
