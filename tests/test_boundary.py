@@ -205,9 +205,9 @@ def test_segmented_fgmres_converges_every_segment_on_its_own():
     b = np.concatenate([rng.normal(size=n) * s for n, s in zip(sizes, (1.0, 1e-6, 1e3))])
     At = torch.as_tensor(A)
     dinv = 1.0 / torch.diagonal(At)
-    seg = torch.repeat_interleave(torch.arange(3), torch.as_tensor(sizes))
+    bounds = np.concatenate([[0], np.cumsum(sizes)])
     x, its, res, ok = segmented_fgmres(lambda v: At @ v, lambda v: dinv * v, torch.as_tensor(b),
-                                       torch.zeros(N, dtype=torch.float64), seg, 3, 1e-8,
+                                       torch.zeros(N, dtype=torch.float64), bounds, 1e-8,
                                        restart=10, maxiter=300)
     assert ok and res <= 1.01e-8
     xe = np.linalg.solve(A, b)

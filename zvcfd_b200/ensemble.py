@@ -54,20 +54,35 @@ def union(meshes: list) -> tuple:
     return Mesh(nodes, elements, zones), offsets, ids
 
 
-def segmented_fgmres(apply_A, apply_M, b, x0, seg, nseg: int, rtol: float, *, restart: int = 30,
+def segmented_fgmres(apply_A, apply_M, b, x0, bounds, rtol: float, *, restart: int = 30,
                      maxiter: int = 200):
     """Right-preconditioned FGMRES with one Krylov recurrence per segment of a block-diagonal
     system: every inner product, norm, Hessenberg column, Givens rotation and step length is
-    taken per segment (``seg``: the segment of each row), while the operator and the
-    preconditioner are applied to all segments at once. Each segment stops by its own
-    criterion, a reduction ``rtol`` of its initial residual (with the reference's round-off
-    floor of ``1e-13`` of its right-hand side); the iteration ends when all have.
-    Returns ``(x, iterations, largest relative residual, all converged)``."""
-    dt = b.dtype
+    taken per segment (``bounds``: the segments' first positions and the end, contiguous),
+    while the operator and the preconditioner are applied to all segments at once. Each segment
+    stops by its own criterion, a reduction ``rtol`` of its initial residual (with the
+    reference's round-off floor of ``1e-13`` of its right-hand side); the iteration ends when
+    all have. The basis is one preallocated ``(restart + 1, n)`` block and each Gram-Schmidt
+    pass is one product per segment, so a Krylov step costs a few launches per segment
+    whatever its index. Returns ``(x, iterations, largest relative residual, all converged)``.
+    """
+    dt, dev = b.dtype, b.device
+    sl = [slice(int(bounds[i]), int(bounds[i + 1])) for i in range(len(bounds) - 1)]
+    nseg = len(sl)
+    n = b.numel()
 
-    def sdot(a, c):
-        return torch.zeros(nseg, dtype=dt, device=b.device).index_add_(0, seg, a * c)
+    def sdot(a, c):                                  # (nseg,) inner products
+        return torch.stack([torch.dot(a[q], c[q]) for q in sl])
 
+    def expand(v):                                   # a value per segment, per row
+        out = torch.empty(n, dtype=dt, device=dev)
+        for i, q in enumerate(sl):
+            out[q] = v[i]
+        return out
+
+    m = restart
+    Vb = torch.zeros((m + 1, n), dtype=dt, device=dev)
+    Zb = torch.zeros((m, n), dtype=dt, device=dev)
     x = x0.clone()
     r = b - apply_A(x)
     beta0 = torch.sqrt(sdot(r, r))
@@ -75,26 +90,25 @@ def segmented_fgmres(apply_A, apply_M, b, x0, seg, nseg: int, rtol: float, *, re
     beta = beta0.clone()
     its = 0
     while its < maxiter and bool((beta > target).any()):
-        m = restart
-        H = torch.zeros((nseg, m + 1, m), dtype=dt, device=b.device)
-        cs = torch.zeros((nseg, m), dtype=dt, device=b.device)
+        H = torch.zeros((nseg, m + 1, m), dtype=dt, device=dev)
+        cs = torch.zeros((nseg, m), dtype=dt, device=dev)
         sn = torch.zeros_like(cs)
-        g = torch.zeros((nseg, m + 1), dtype=dt, device=b.device)
+        g = torch.zeros((nseg, m + 1), dtype=dt, device=dev)
         g[:, 0] = beta
-        V = [r * torch.where(beta > 0, 1.0 / beta, torch.zeros_like(beta))[seg]]
-        Z = []
+        Vb[0] = r * expand(torch.where(beta > 0, 1.0 / beta, torch.zeros_like(beta)))
         k_used = 0
         for k in range(m):
-            Z.append(apply_M(V[k]))
-            w = apply_A(Z[k])
+            Zb[k] = apply_M(Vb[k])
+            w = apply_A(Zb[k])
+            V = Vb[:k + 1]
             for _ in range(2):                                   # classical Gram-Schmidt, twice
-                h = torch.stack([sdot(V[j], w) for j in range(k + 1)])      # (k+1, nseg)
-                for j in range(k + 1):
-                    w = w - h[j][seg] * V[j]
+                h = torch.stack([V[:, q] @ w[q] for q in sl], 1)          # (k+1, nseg)
+                for i, q in enumerate(sl):
+                    w[q] -= h[:, i] @ V[:, q]
                 H[:, :k + 1, k] += h.T
             hn = torch.sqrt(sdot(w, w))
             H[:, k + 1, k] = hn
-            V.append(w * torch.where(hn > 0, 1.0 / hn, torch.zeros_like(hn))[seg])
+            Vb[k + 1] = w * expand(torch.where(hn > 0, 1.0 / hn, torch.zeros_like(hn)))
             for j in range(k):                                   # earlier rotations
                 t = cs[:, j] * H[:, j, k] + sn[:, j] * H[:, j + 1, k]
                 H[:, j + 1, k] = -sn[:, j] * H[:, j, k] + cs[:, j] * H[:, j + 1, k]
@@ -116,9 +130,9 @@ def segmented_fgmres(apply_A, apply_M, b, x0, seg, nseg: int, rtol: float, *, re
         zero = R.diagonal(dim1=1, dim2=2) == 0                  # segments with nothing to solve
         R.diagonal(dim1=1, dim2=2)[zero] = 1.0
         rhs[zero] = 0.0
-        y = torch.linalg.solve_triangular(R, rhs[..., None], upper=True)[..., 0]
-        for j in range(k_used):
-            x = x + y[:, j][seg] * Z[j]
+        y = torch.linalg.solve_triangular(R, rhs[..., None], upper=True)[..., 0]   # (nseg, k)
+        for i, q in enumerate(sl):
+            x[q] += y[i] @ Zb[:k_used, q]
         r = b - apply_A(x)
         beta = torch.sqrt(sdot(r, r))
     rel = beta / torch.where(beta0 > 0, beta0, torch.ones_like(beta0))
@@ -130,18 +144,17 @@ class SegmentedKrylov:
     on the union: block-diagonal, since its aggregates never cross instances) preconditions
     :func:`segmented_fgmres` with one Krylov recurrence per instance (``krylov="segmented"``).
 
-    Experimental: the recurrences run in Python over torch tensors (tens of small launches and
-    a host read-back per Krylov step), and its one GPU run, the three-vessel ensemble test,
-    exceeded its 200 s limit; the algorithm itself is checked on the CPU. It is the shape of
-    the per-instance recurrences the union solve needs, to be moved into the device FGMRES."""
+    Experimental: the recurrences run as torch operations (a few launches per instance and a
+    host read-back per Krylov step); an earlier form, with launches growing with the Krylov
+    index, exceeded 200 s on the three-vessel ensemble test; the algorithm is checked on the
+    CPU. It is the shape of the per-instance recurrences the union solve needs, to be moved
+    into the device FGMRES."""
 
     name = "b200-segmented"
 
     def __init__(self, offsets, amg, *, restart: int = 30, maxiter: int = 200):
         self.amg, self.restart, self.maxiter = amg, restart, maxiter
-        counts = torch.as_tensor(np.diff(offsets) * 4, device="cuda")
-        self.seg = torch.repeat_interleave(torch.arange(len(counts), device="cuda"), counts)
-        self.nseg = len(counts)
+        self.bounds = [4 * int(o) for o in offsets]
         self.rtol = amg.rtol
 
     def solve(self, A, b, x0=None, rtol=None):
@@ -151,7 +164,7 @@ class SegmentedKrylov:
         t = time.time()
         b = b.reshape(-1).contiguous()
         x0 = torch.zeros_like(b) if x0 is None else x0.reshape(-1).contiguous()
-        x, its, res, ok = segmented_fgmres(A.matvec, self.amg.vcycle, b, x0, self.seg, self.nseg,
+        x, its, res, ok = segmented_fgmres(A.matvec, self.amg.vcycle, b, x0, self.bounds,
                                            self.rtol if rtol is None else rtol,
                                            restart=self.restart, maxiter=self.maxiter)
         torch.cuda.synchronize()
