@@ -14,7 +14,8 @@ pipe (``transient``); wall shear (``wall``); the 0-D RCR model, BDF
 coefficients and Carreau-Yasuda viscosity (``lumped``); the backflow box with
 and without stabilisation (``backflow``); zone forces, flows and both wall-shear
 methods of two converged cases (``forces``); WSS time statistics (``wss``);
-the manufactured Carreau-Yasuda outlet (``gn_outlet``). A single file is
+the manufactured Carreau-Yasuda outlet (``gn_outlet``); developed inlet
+profiles and a pipe with the default flow-rate inlet (``profiles``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -394,6 +395,38 @@ def gn_outlet_case() -> dict:
                 f=src, J=J, iterations=rep.iterations)
 
 
+def profiles_case() -> dict:
+    """The developed inlet profile (``zvcfd/fv/profiles.py``) on four inlet faces (a mixed
+    quad/triangle circle, a triangulated circle, a quad and a triangulated rectangle), and a
+    pipe with a flow-rate inlet of the default profile solved by the reference's CPU solver."""
+    from zvcfd.fv.profiles import poiseuille, shape
+
+    out = {}
+    meshes = {"tube_mixed": tube(0.5, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed",
+                                 layers=1),
+              "tube_tet": tube(1.0, 2.0, n_core=3, n_ring=3, n_axial=4, kind="tet"),
+              "box_hex": box((5, 4, 3), (1.0, 0.7, 0.4), kind="hex"),
+              "box_tet": box((5, 4, 3), (1.0, 0.7, 0.4), kind="tet", warp=0.03)}
+    for tag, m in meshes.items():
+        z = next(zz for zz in m.zones.values() if zz.name in ("inlet", "xmin"))
+        u = poiseuille(m.nodes, z.faces)
+        nodes, v = shape(m.nodes, z.faces, "poiseuille")
+        out.update({f"{tag}_X": m.nodes, f"{tag}_faces": z.faces, f"{tag}_nodes": nodes,
+                    f"{tag}_u": np.array([u[int(g)] for g in nodes]), f"{tag}_shape": v})
+    m = meshes["tube_mixed"]
+    zid = {zz.name: k for k, zz in m.zones.items()}
+    bcs = {zid["inlet"]: {"kind": "velocity", "flow_rate": 0.3},
+           zid["outlet"]: {"kind": "pressure", "value": 0.0}, zid["wall"]: {"kind": "wall"}}
+    s = ReferenceSolver(m, Fluid(1.0, 0.2), bcs, advection=1.0)
+    rep = s.solve(max_iterations=300, tol=1e-13)
+    assert rep.converged
+    for k, v in mesh_arrays(m).items():
+        out[f"pipe_{k}"] = v
+    out.update(pipe_U=s.U.copy(), pipe_P=s.P.copy(), pipe_flow_rate=0.3, pipe_rho=1.0,
+               pipe_mu=0.2)
+    return out
+
+
 def lumped_case() -> dict:
     """The reference's RCR model (``zvcfd/lumped.py:181-218``): steady coefficients, and the
     step coefficients and committed pressures of 40 steps under a pulsatile outflow, for the
@@ -434,6 +467,10 @@ def lumped_case() -> dict:
 
 
 def main():
+    if sys.argv[1:] == ["profiles"]:
+        np.savez_compressed(HERE / "profiles.npz", **profiles_case())
+        print("wrote profiles")
+        return
     if sys.argv[1:] == ["gn_outlet"]:
         np.savez_compressed(HERE / "gn_outlet.npz", **gn_outlet_case())
         print("wrote gn_outlet")
@@ -490,6 +527,8 @@ def main():
     print("wrote wss")
     np.savez_compressed(HERE / "gn_outlet.npz", **gn_outlet_case())
     print("wrote gn_outlet")
+    np.savez_compressed(HERE / "profiles.npz", **profiles_case())
+    print("wrote profiles")
 
 
 if __name__ == "__main__":
