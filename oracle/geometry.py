@@ -52,31 +52,35 @@ def gradients(x: np.ndarray, kind: str) -> np.ndarray:
 
 
 def boundary_subfaces(nodes: np.ndarray, faces: np.ndarray) -> np.ndarray:
-    """Each node's share of each boundary face, area vectors ``(F, 4, 3)`` (``geometry.py:226-244``)."""
-    tri = faces[:, 3] < 0
+    """Each node's share of each boundary face, area vectors ``(F, 4, 3)`` (``geometry.py:226-244``):
+    the polygon node, next edge midpoint, face centroid, previous edge midpoint, by the vector
+    shoelace formula, one face at a time."""
     out = np.zeros(faces.shape + (3,))
-    for n, sel in ((3, tri), (4, ~tri)):
-        if not sel.any():
-            continue
-        p = nodes[faces[sel, :n]]
-        fc = p.mean(1)
-        rows = np.flatnonzero(sel)
+    for fi, face in enumerate(faces):
+        P = nodes[[int(v) for v in face if v >= 0]]
+        n = len(P)
+        c = P.mean(0)
         for i in range(n):
-            nxt = 0.5 * (p[:, i] + p[:, (i + 1) % n])
-            prv = 0.5 * (p[:, i] + p[:, (i - 1) % n])
-            out[rows, i] = 0.5 * np.cross(fc - p[:, i], prv - nxt)
+            # taken about the centroid, so that far-off coordinates cost no precision
+            poly = [P[i] - c, 0.5 * (P[i] + P[(i + 1) % n]) - c, np.zeros(3),
+                    0.5 * (P[i] + P[(i - 1) % n]) - c]
+            out[fi, i] = 0.5 * sum(np.cross(poly[k], poly[(k + 1) % 4]) for k in range(4))
     return out
 
 
 def boundary_subface_weights(faces: np.ndarray) -> np.ndarray:
-    """Weights ``(F, 4, 4)`` from face nodes to each sub-face's area centroid (``geometry.py:247-266``)."""
-    tri = faces[:, 3] < 0
+    """Weights ``(F, 4, 4)`` from face nodes to each sub-face's area centroid (``geometry.py:247-266``):
+    22/36 for the node and 7/36 for each other on a triangle; on a quadrilateral 9/16, 3/16, 1/16
+    by the distance around the face."""
+    tri = (15.0 * np.eye(3) + 7.0) / 36.0
+    gap = np.abs(np.subtract.outer(np.arange(4), np.arange(4)))
+    quad = np.array([9.0, 3.0, 1.0])[np.minimum(gap, 4 - gap)] / 16.0
     w = np.zeros(faces.shape + (4,))
-    t = np.full((3, 3), 7.0 / 36.0)
-    np.fill_diagonal(t, 11.0 / 18.0)
-    q = np.array([[9, 3, 1, 3], [3, 9, 3, 1], [1, 3, 9, 3], [3, 1, 3, 9]]) / 16.0
-    w[tri, :3, :3] = t
-    w[~tri] = q
+    for fi, face in enumerate(faces):
+        if face[3] >= 0:
+            w[fi] = quad
+        else:
+            w[fi, :3, :3] = tri
     return w
 
 
