@@ -46,42 +46,48 @@ class Zone:
 
 @dataclass
 class Mesh:
+    """Nodes ``(N, 3)``, elements ``{kind: (E, n)}`` and boundary zones ``{id: Zone}``."""
+
     nodes: np.ndarray
     elements: dict
     zones: dict = field(default_factory=dict)
 
     def __post_init__(self):
-        self.nodes = np.ascontiguousarray(self.nodes, np.float64)
-        self.elements = {k: np.ascontiguousarray(self.elements[k], np.int64)
-                         for k in KINDS if k in self.elements and len(self.elements[k])}
+        self.nodes = np.require(self.nodes, np.float64, "C")
+        kept = {}
+        for kind in KINDS:                       # canonical order, empty types dropped
+            e = self.elements.get(kind)
+            if e is not None and len(e):
+                kept[kind] = np.require(e, np.int64, "C")
+        self.elements = kept
 
     @property
     def n_nodes(self) -> int:
-        return len(self.nodes)
+        return self.nodes.shape[0]
 
     @property
     def n_elements(self) -> int:
-        return sum(len(e) for e in self.elements.values())
+        return int(sum(e.shape[0] for e in self.elements.values()))
 
     def zone_id(self, name: str) -> int:
-        for zid, z in self.zones.items():
-            if z.name == name:
-                return zid
-        raise KeyError(name)
+        found = [zid for zid, z in self.zones.items() if z.name == name]
+        if not found:
+            raise KeyError(name)
+        return found[0]
 
     def element_volumes(self, kind: str) -> np.ndarray:
-        """Volume of each element, every face fanned about its centroid."""
-        e = self.elements[kind]
-        x = self.nodes[e]
-        c = x.mean(1)
-        vol = np.zeros(len(e))
-        for f in FACES[kind]:
-            p = x[:, list(f)]
-            fc = p.mean(1)
-            for i in range(len(f)):
-                a, b = p[:, i], p[:, (i + 1) % len(f)]
-                vol += np.einsum("ij,ij->i", np.cross(a - fc, b - fc), c - fc) / 6.0
-        return -vol
+        """Volume of each element: the tetrahedra joining the element's centroid to every
+        face, each face fanned about its own centroid (outward faces give negative signed
+        volumes, hence the sign)."""
+        x = self.nodes[self.elements[kind]]
+        centre = x.mean(1)
+        vol = np.zeros(len(x))
+        for face in FACES[kind]:
+            ring = x[:, list(face)]
+            mid = ring.mean(1)
+            for a, b in zip(ring.transpose(1, 0, 2), np.roll(ring, -1, axis=1).transpose(1, 0, 2)):
+                vol -= np.einsum("ij,ij->i", np.cross(a - mid, b - mid), centre - mid) / 6.0
+        return vol
 
     def boundary_faces(self) -> np.ndarray:
         """Faces ``(F, 4)`` that belong to one element only, outward."""
@@ -114,132 +120,159 @@ class Mesh:
 
 # ---------------------------------------------------------------- splitting
 
-# Dompierre et al. (1999), table 2: vertex permutations taking each vertex of a
-# wedge to position 0 while keeping the wedge's topology (bottom 0 1 2, top 3 4 5)
-_WEDGE_ROT = np.array([[0, 1, 2, 3, 4, 5], [1, 2, 0, 4, 5, 3], [2, 0, 1, 5, 3, 4],
-                       [3, 5, 4, 0, 2, 1], [4, 3, 5, 1, 0, 2], [5, 4, 3, 2, 1, 0]])
+def _wedge_symmetries() -> np.ndarray:
+    """Row ``v``: the relabelling of a wedge (triangle 0 1 2 under triangle 3 4 5) that brings
+    local vertex ``v`` to position 0 and keeps the element's orientation: a rotation of both
+    triangles, for a top vertex with the triangles exchanged and their direction reversed
+    (the vertex permutations of Dompierre et al. 1999, table 2)."""
+    rows = []
+    for v in range(6):
+        r = v % 3
+        if v < 3:
+            tri = [r, (r + 1) % 3, (r + 2) % 3]
+            rows.append(tri + [3 + i for i in tri])
+        else:
+            tri = [r, (r + 2) % 3, (r + 1) % 3]
+            rows.append([3 + i for i in tri] + tri)
+    return np.array(rows)
+
+
+_WEDGE_SYM = _wedge_symmetries()
+# the three tetrahedra of a wedge relabelled so that vertex 0 holds its smallest index, for
+# either diagonal of the quadrilateral 1-2-5-4 opposite that vertex
+_TETS_CUT_15 = np.array([[0, 1, 2, 5], [0, 1, 5, 4], [0, 4, 5, 3]])
+_TETS_CUT_24 = np.array([[0, 1, 2, 4], [0, 4, 2, 5], [0, 4, 5, 3]])
 
 
 def split_wedges(w: np.ndarray) -> np.ndarray:
-    """Three tetrahedra per wedge, conforming by the smallest-global-index rule."""
+    """Three tetrahedra per wedge, conforming: each quadrilateral is cut along the diagonal
+    through its smallest global index, so the two elements sharing it cut it alike."""
     w = np.asarray(w, np.int64)
-    p = w[np.arange(len(w))[:, None], _WEDGE_ROT[np.argmin(w, axis=1)]]
-    v = [p[:, i] for i in range(6)]
-    # the quad (1, 2, 5, 4) opposite vertex 0 is cut through its smallest vertex
-    cut15 = np.minimum(v[1], v[5]) < np.minimum(v[2], v[4])
-    t = np.empty((len(w), 3, 4), np.int64)
-    t[:, 0] = np.where(cut15[:, None], np.stack([v[0], v[1], v[2], v[5]], 1),
-                       np.stack([v[0], v[1], v[2], v[4]], 1))
-    t[:, 1] = np.where(cut15[:, None], np.stack([v[0], v[1], v[5], v[4]], 1),
-                       np.stack([v[0], v[4], v[2], v[5]], 1))
-    t[:, 2] = np.stack([v[0], v[4], v[5], v[3]], 1)
-    return t.reshape(-1, 4)
+    rows = np.arange(len(w))[:, None]
+    lab = w[rows, _WEDGE_SYM[np.argmin(w, axis=1)]]
+    cut15 = np.minimum(lab[:, 1], lab[:, 5]) < np.minimum(lab[:, 2], lab[:, 4])
+    local = np.where(cut15[:, None, None], _TETS_CUT_15, _TETS_CUT_24)
+    return lab[rows[:, :, None], local].reshape(-1, 4)
 
 
 def split_hexes(h: np.ndarray) -> np.ndarray:
-    """Two wedges per hexahedron (triangles on faces 0-3 and 4-7), both cut along the
-    diagonal through the bottom quad's smallest node. Columns of hexahedra numbered
-    the same way layer after layer therefore stay conforming."""
+    """Two wedges per hexahedron with their triangles on faces 0-1-2-3 and 4-5-6-7, both cut
+    along the diagonal through the bottom quadrilateral's smallest node. Columns of
+    hexahedra numbered the same way layer after layer therefore stay conforming."""
     h = np.asarray(h, np.int64)
-    b = h[:, :4]
-    diag13 = np.argmin(np.minimum(b[:, [0, 1, 2, 3]], b[:, [2, 3, 0, 1]]), axis=1) % 2
-    sel = np.where(diag13[:, None] == 0, np.array([[0, 1, 2, 0, 2, 3]]),
-                   np.array([[0, 1, 3, 1, 2, 3]]))
-    r = np.arange(len(h))[:, None]
-    bot, top = b[r, sel], h[:, 4:][r, sel]
-    w1 = np.concatenate([bot[:, :3], top[:, :3]], 1)
-    w2 = np.concatenate([bot[:, 3:], top[:, 3:]], 1)
-    return np.stack([w1, w2], 1).reshape(-1, 6)
+    through13 = np.argmin(h[:, :4], axis=1) % 2 == 1
+    halves = np.where(through13[:, None, None], np.array([[0, 1, 3], [1, 2, 3]]),
+                      np.array([[0, 1, 2], [0, 2, 3]]))
+    rows = np.arange(len(h))[:, None, None]
+    return np.concatenate([h[rows, halves], h[rows, halves + 4]], axis=2).reshape(-1, 6)
+
+
+# per kind: the three edges from local node 0 whose triple product is the volume's sign, and
+# the mirror relabelling that reverses it
+_ORIENTATION = {"tet": ([1, 2, 3], [0, 2, 1, 3]), "wedge": ([1, 2, 3], [0, 2, 1, 3, 5, 4]),
+                "hex": ([1, 3, 4], [0, 3, 2, 1, 4, 7, 6, 5])}
 
 
 def orient(nodes: np.ndarray, kind: str, e: np.ndarray) -> np.ndarray:
     """Reorder each element's local nodes so that its volume is positive."""
     e = np.array(e, np.int64)
-    x = nodes[e]
-    if kind in ("tet", "wedge"):
-        s = np.einsum("ij,ij->i", np.cross(x[:, 1] - x[:, 0], x[:, 2] - x[:, 0]),
-                      x[:, 3] - x[:, 0])
-        perm = [0, 2, 1, 3] if kind == "tet" else [0, 2, 1, 3, 5, 4]
-    elif kind == "hex":
-        s = np.einsum("ij,ij->i", np.cross(x[:, 1] - x[:, 0], x[:, 3] - x[:, 0]),
-                      x[:, 4] - x[:, 0])
-        perm = [0, 3, 2, 1, 4, 7, 6, 5]
-    else:
+    if kind not in _ORIENTATION:
         return e
-    e[s < 0] = e[s < 0][:, perm]
+    edges, mirror = _ORIENTATION[kind]
+    x = nodes[e]
+    d = x[:, edges] - x[:, :1]
+    neg = np.einsum("ij,ij->i", d[:, 0], np.cross(d[:, 1], d[:, 2])) < 0
+    e[neg] = e[neg][:, mirror]
     return e
 
 
 def _zones(mesh: Mesh, classify, names) -> dict:
+    """Zones 3, 4, ... named ``names[i] = (name, kind)``: the boundary faces ``classify``
+    (from their centroids and unit normals) assigns to ``i``; every face must be assigned."""
     f = mesh.boundary_faces()
-    p = mesh.nodes[np.where(f < 0, f[:, :1], f)]
-    tri = f[:, 3] < 0
-    c = np.where(tri[:, None], p[:, :3].mean(1), p.mean(1))
-    nrm = np.where(tri[:, None], np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]),
-                   np.cross(p[:, 2] - p[:, 0], p[:, 3] - p[:, 1]))
-    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
-    which = classify(c, nrm)
-    zones = {}
-    for i, (name, kind) in enumerate(names):
-        zones[3 + i] = Zone(3 + i, kind, name, f[which == i])
-    if sum(z.n_faces for z in zones.values()) != len(f):
+    quad = f[:, 3] >= 0
+    P = mesh.nodes[np.where(f >= 0, f, f[:, :1])]
+    centre = np.where(quad[:, None], P.mean(1), P[:, :3].mean(1))
+    # twice the polygon's area vector, about its centroid: a triangle's pad repeats vertex 0,
+    # which closes its loop and adds nothing
+    rel = P - centre[:, None]
+    area = np.cross(rel, np.roll(rel, -1, axis=1)).sum(1)
+    normal = area / np.linalg.norm(area, axis=1, keepdims=True)
+    which = classify(centre, normal)
+    if np.any(which < 0) or np.any(which >= len(names)):
         raise ValueError("unclassified boundary faces")
-    return zones
+    return {3 + i: Zone(3 + i, kind, name, f[which == i]) for i, (name, kind) in enumerate(names)}
 
 
 def jitter(mesh: Mesh, amount: float, seed: int) -> None:
     """Move interior nodes at random by up to ``amount`` times their shortest edge."""
     if not amount:
         return
+    from zvcfd_b200.topology import EDGES
+
     rng = np.random.default_rng(seed)
-    bnd = np.zeros(mesh.n_nodes, bool)
+    fixed = np.zeros(mesh.n_nodes, bool)
     for z in mesh.zones.values():
-        bnd[z.faces[z.faces >= 0]] = True
-    h = np.full(mesh.n_nodes, np.inf)
+        fixed[z.faces[z.faces >= 0]] = True
+    shortest = np.full(mesh.n_nodes, np.inf)
     for kind, e in mesh.elements.items():
-        from zvcfd_b200.topology import EDGES
         for a, b in EDGES[kind]:
-            ln = np.linalg.norm(mesh.nodes[e[:, b]] - mesh.nodes[e[:, a]], axis=1)
-            np.minimum.at(h, e[:, a], ln)
-            np.minimum.at(h, e[:, b], ln)
-    d = rng.uniform(-1.0, 1.0, (mesh.n_nodes, 3)) * (amount * h)[:, None]
-    d[bnd] = 0.0
-    mesh.nodes = mesh.nodes + d
-    for k in mesh.elements:
-        if (mesh.element_volumes(k) <= 0).any():
-            raise ValueError("the jitter inverted an element; use a smaller amount")
+            length = np.linalg.norm(mesh.nodes[e[:, b]] - mesh.nodes[e[:, a]], axis=1)
+            np.minimum.at(shortest, e[:, a], length)
+            np.minimum.at(shortest, e[:, b], length)
+    move = rng.uniform(-1.0, 1.0, (mesh.n_nodes, 3)) * (amount * shortest)[:, None]
+    move[fixed] = 0.0
+    mesh.nodes = mesh.nodes + move
+    if any((mesh.element_volumes(k) <= 0).any() for k in mesh.elements):
+        raise ValueError("the jitter inverted an element; use a smaller amount")
 
 
 # ---------------------------------------------------------------- generators
 
+# VTK corner order of a hexahedral lattice cell, as offsets (i, j, k)
+_CELL_CORNERS = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                          [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+
+
 def box(n=(4, 4, 4), lengths=(1.0, 1.0, 1.0), *, kind: str = "hex", perturb: float = 0.0,
         seed: int = 0) -> Mesh:
     """A structured box; zones 3-8 ``xmin xmax ymin ymax zmin zmax`` (walls)."""
-    nx, ny, nz = n
-    xs = [np.linspace(0.0, L, k + 1) for L, k in zip(lengths, n)]
-    X, Y, Z = np.meshgrid(*xs, indexing="ij")
-    nodes = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
-    idx = np.arange(len(nodes)).reshape(nx + 1, ny + 1, nz + 1)
-    i, j, k = (a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz),
-                                              indexing="ij"))
-    hexes = np.stack([idx[i, j, k], idx[i + 1, j, k], idx[i + 1, j + 1, k], idx[i, j + 1, k],
-                      idx[i, j, k + 1], idx[i + 1, j, k + 1], idx[i + 1, j + 1, k + 1],
-                      idx[i, j + 1, k + 1]], 1)
-    els = {"hex": hexes} if kind == "hex" else {"wedge": split_hexes(hexes)} \
-        if kind == "wedge" else {"tet": split_wedges(split_hexes(hexes))}
+    n = np.asarray(n, np.int64)
+    axes = [np.linspace(0.0, L, k + 1) for L, k in zip(lengths, n)]
+    lattice = np.indices(n + 1).reshape(3, -1).T            # (i, j, k), k fastest
+    nodes = np.stack([axes[d][lattice[:, d]] for d in range(3)], 1)
+    cells = np.indices(n).reshape(3, -1).T
+    c = cells[:, None, :] + _CELL_CORNERS[None]
+    hexes = (c[..., 0] * (n[1] + 1) + c[..., 1]) * (n[2] + 1) + c[..., 2]
+    if kind == "hex":
+        els = {"hex": hexes}
+    elif kind == "wedge":
+        els = {"wedge": split_hexes(hexes)}
+    else:
+        els = {"tet": split_wedges(split_hexes(hexes))}
     mesh = Mesh(nodes, {k: orient(nodes, k, v) for k, v in els.items()})
     tol = 1e-9 * max(lengths)
+    planes = [(ax, side * lengths[ax]) for ax in range(3) for side in (0, 1)]
 
-    def classify(c, nrm):
-        w = np.full(len(c), -1)
-        for s, (ax, side) in enumerate([(0, 0), (0, 1), (1, 0), (1, 1), (2, 0), (2, 1)]):
-            w[np.abs(c[:, ax] - side * lengths[ax]) < tol] = s
+    def classify(centre, normal):
+        w = np.full(len(centre), -1)
+        for i, (ax, at) in enumerate(planes):
+            w[np.abs(centre[:, ax] - at) < tol] = i
         return w
 
     mesh.zones = _zones(mesh, classify, [(nm, "wall") for nm in
                                          ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")])
     jitter(mesh, perturb, seed)
     return mesh
+
+
+def _grid_quads(first: int, rows: int, cols: int) -> np.ndarray:
+    """The quadrilaterals of a ``rows x cols`` cell grid whose ``(rows + 1) x (cols + 1)``
+    nodes are numbered row by row from ``first``: corners (r, c), (r+1, c), (r+1, c+1),
+    (r, c+1)."""
+    r, c = (v.reshape(-1) for v in np.indices((rows, cols)))
+    at = lambda rr, cc: first + rr * (cols + 1) + cc            # noqa: E731
+    return np.stack([at(r, c), at(r + 1, c), at(r + 1, c + 1), at(r, c + 1)], 1)
 
 
 def ogrid_section(radius: float, n_core: int, n_ring: int, *, core: float = 0.5,
@@ -251,42 +284,43 @@ def ogrid_section(radius: float, n_core: int, n_ring: int, *, core: float = 0.5,
     Each outer block's radial cells grow by ``growth`` from the core outward
     (``growth < 1`` makes the wall cells thinnest).
     """
-    half = core * radius / np.sqrt(2.0)
-    t = np.linspace(-1.0, 1.0, n_core + 1)
-    w = growth ** np.arange(n_ring)
-    frac = np.r_[0.0, np.cumsum(w) / w.sum()]
-    pts, quads, layer = [], [], []
-    gx, gy = np.meshgrid(t, t, indexing="ij")
-    pts.append(np.stack([half * gx.ravel(), half * gy.ravel()], 1))
-    ci = np.arange((n_core + 1) ** 2).reshape(n_core + 1, n_core + 1)
-    a, b = (v.ravel() for v in np.meshgrid(np.arange(n_core), np.arange(n_core), indexing="ij"))
-    quads.append(np.stack([ci[a, b], ci[a + 1, b], ci[a + 1, b + 1], ci[a, b + 1]], 1))
-    layer.append(np.full(len(a), -1))
-    base = (n_core + 1) ** 2
+    half = core * radius / np.sqrt(2.0)          # half the side of the core square
+    s = np.linspace(-1.0, 1.0, n_core + 1)       # position along a side, or along an arc
+    cell = growth ** np.arange(n_ring)
+    frac = np.r_[0.0, np.cumsum(cell) / cell.sum()]
+    xs, ys = np.meshgrid(half * s, half * s, indexing="ij")
+    pts = [np.stack([xs.reshape(-1), ys.reshape(-1)], 1)]
+    quads = [_grid_quads(0, n_core, n_core)]
+    layer = [np.full(n_core * n_core, -1)]
+    first = len(pts[0])
+    # block q: from the core side x = half to the arc of +-45 degrees about the +x axis,
+    # turned by q right angles
+    inner = np.stack([np.full(n_core + 1, half), half * s], 1)
+    outer = radius * np.stack([np.cos(s * np.pi / 4), np.sin(s * np.pi / 4)], 1)
+    block = (1.0 - frac)[:, None, None] * inner[None] + frac[:, None, None] * outer[None]
     for q in range(4):
-        c, s = np.cos(q * np.pi / 2), np.sin(q * np.pi / 2)
-        rot = np.array([[c, -s], [s, c]])
-        side = np.stack([np.full_like(t, half), half * t], 1)
-        ang = t * np.pi / 4
-        arc = radius * np.stack([np.cos(ang), np.sin(ang)], 1)
-        blk = (1.0 - frac[:, None, None]) * side[None] + frac[:, None, None] * arc[None]
-        pts.append(blk.reshape(-1, 2) @ rot.T)
-        bi = base + np.arange((n_ring + 1) * (n_core + 1)).reshape(n_ring + 1, n_core + 1)
-        a, b = (v.ravel() for v in np.meshgrid(np.arange(n_ring), np.arange(n_core),
-                                               indexing="ij"))
-        quads.append(np.stack([bi[a, b], bi[a + 1, b], bi[a + 1, b + 1], bi[a, b + 1]], 1))
-        layer.append(n_ring - 1 - a)
-        base += bi.size
-    xy = np.concatenate(pts)
-    quads = np.concatenate(quads)
-    layer = np.concatenate(layer)
-    # merge the nodes the blocks share, keeping first occurrences in order
-    key = np.round(xy / (radius * 1e-9)).astype(np.int64)
-    _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
-    inv = inv.reshape(-1)
-    renum = np.empty(len(first), np.int64)
-    renum[np.argsort(first)] = np.arange(len(first))
-    return xy[np.sort(first)], renum[inv[quads]], layer
+        c, sn = np.cos(q * np.pi / 2), np.sin(q * np.pi / 2)
+        turn = np.array([[c, -sn], [sn, c]])
+        pts.append(block.reshape(-1, 2) @ turn.T)
+        quads.append(_grid_quads(first, n_ring, n_core))
+        layer.append(np.repeat(n_ring - 1 - np.arange(n_ring), n_core))
+        first += (n_ring + 1) * (n_core + 1)
+    xy, quads, layer = np.concatenate(pts), np.concatenate(quads), np.concatenate(layer)
+    # merge the nodes two blocks share, numbered in order of first appearance
+    keys = np.round(xy / (radius * 1e-9)).astype(np.int64)
+    number, new_id = {}, np.empty(len(xy), np.int64)
+    for i, k in enumerate(map(tuple, keys)):
+        new_id[i] = number.setdefault(k, len(number))
+    kept = np.zeros(len(number), np.int64)
+    kept[new_id[::-1]] = np.arange(len(xy))[::-1]                # first occurrence of each
+    return xy[kept], new_id[quads], layer
+
+
+def _sweep(quads: np.ndarray, per: int, n_axial: int) -> np.ndarray:
+    """``(n_axial, Q, 8)``: the hexahedra between consecutive copies (``per`` nodes apart) of
+    a section's quadrilaterals."""
+    lower = quads[None] + (per * np.arange(n_axial))[:, None, None]
+    return np.concatenate([lower, lower + per], axis=2)
 
 
 def pipe(radius: float = 1e-3, length: float = 10e-3, *, n_core: int = 14, n_ring: int = 7,
@@ -295,11 +329,9 @@ def pipe(radius: float = 1e-3, length: float = 10e-3, *, n_core: int = 14, n_rin
     """A straight circular pipe along z. Zones: 3 ``inlet`` (z = 0), 4 ``outlet``
     (z = length), 5 ``wall``. ``kind``: ``"tet"`` (six per hexahedron) or ``"hex"``."""
     xy, quads, _ = ogrid_section(radius, n_core, n_ring, growth=growth)
-    P = len(xy)
     z = np.linspace(0.0, length, n_axial + 1)
-    nodes = np.concatenate([np.column_stack([xy, np.full(P, zk)]) for zk in z])
-    k = np.arange(n_axial)[:, None, None] * P
-    hexes = np.concatenate([quads[None] + k, quads[None] + k + P], axis=2).reshape(-1, 8)
+    nodes = np.column_stack([np.tile(xy, (n_axial + 1, 1)), np.repeat(z, len(xy))])
+    hexes = _sweep(quads, len(xy), n_axial).reshape(-1, 8)
     els = {"hex": hexes} if kind == "hex" else {"tet": split_wedges(split_hexes(hexes))}
     mesh = Mesh(nodes, {kk: orient(nodes, kk, v) for kk, v in els.items()})
     tol = 1e-9 * max(radius, length)
@@ -330,7 +362,6 @@ def curved_tube(radius: float = 2e-3, bend: float = 20e-3, angle: float = np.pi 
     if bend <= radius:
         raise ValueError("the bend radius must exceed the tube radius")
     xy, quads, layer = ogrid_section(radius, n_core, n_ring, growth=growth)
-    P = len(xy)
     th = np.linspace(0.0, angle, n_axial + 1)
     rows = []
     for t in th:
@@ -338,8 +369,7 @@ def curved_tube(radius: float = 2e-3, bend: float = 20e-3, angle: float = np.pi 
         ex = np.array([np.cos(t), 0.0, -np.sin(t)])
         rows.append(ctr[None] + xy[:, :1] * ex[None] + xy[:, 1:2] * np.array([[0.0, 1.0, 0.0]]))
     nodes = np.concatenate(rows)
-    k = np.arange(n_axial)[:, None, None] * P
-    hexes = np.concatenate([quads[None] + k, quads[None] + k + P], axis=2)
+    hexes = _sweep(quads, len(xy), n_axial)
     wall = (layer >= 0) & (layer < layers)
     els = {"hex": hexes[:, ~wall].reshape(-1, 8),
            "wedge": split_hexes(hexes[:, wall].reshape(-1, 8))}
