@@ -50,6 +50,27 @@ class RawRows:
         return torch.where(self.kept[:, None], r - self.b, torch.zeros_like(r))
 
 
+def _zone_areas(bc, zid) -> np.ndarray:
+    """``(N,)``: each node's sub-face area in zone ``zid``."""
+    f, S = bc.sub[zid]
+    ok = f >= 0
+    return np.bincount(f[ok], np.linalg.norm(S[ok], axis=-1), bc.N)
+
+
+def _fixed_axes(bc, zid) -> np.ndarray:
+    """The velocity components a zone fixes: all three, or a symmetry plane's normal axis."""
+    if bc.bcs[zid]["kind"] != "symmetry":
+        return np.ones(3, bool)
+    total = np.abs(bc.sub[zid][1].reshape(-1, 3).sum(0))
+    return total == total.max()
+
+
+def _inlet_momentum(bc, zid) -> np.ndarray:
+    """``(3,)``: the momentum flux ``Σ m_sub u_sub`` through a zone's sub-faces."""
+    f = bc.sub[zid][0]
+    return np.einsum("fi,fik->k", np.where(f >= 0, bc.sub_flow[zid], 0.0), bc.sub_vel[zid])
+
+
 def zone_forces(bc, residual: np.ndarray, P: np.ndarray, *, stokes: bool = False,
                 lumped=()) -> dict:
     """Force of the fluid on each zone, ``{zone: (3,)}`` (N).
@@ -68,35 +89,25 @@ def zone_forces(bc, residual: np.ndarray, P: np.ndarray, *, stokes: bool = False
         stokes: no advection (no momentum carried through inlets).
         lumped: ids of the lumped pressure zones.
     """
-    N = bc.N
-    react = np.where(bc.vel_fixed_comp, -np.asarray(residual)[:, :3], 0.0)
-    per, tot = {}, np.zeros((N, 3))
-    for zid, (f, S) in bc.sub.items():
-        kind = bc.bcs[zid]["kind"]
-        if kind == "pressure":
-            continue
-        ok = f >= 0
-        a = np.bincount(f[ok], np.linalg.norm(S, axis=2)[ok], N)
-        comp = np.ones(3, bool)
-        if kind == "symmetry":
-            sn = np.abs(S.reshape(-1, 3).sum(0))
-            comp = sn == sn.max()
-        per[zid] = a[:, None] * comp[None, :]
-        tot += per[zid]
+    reaction = -np.where(bc.vel_fixed_comp, np.asarray(residual)[:, :3], 0.0)
+    fixing = [z for z in bc.sub if bc.bcs[z]["kind"] != "pressure"]
+    # (zones, N, 3): each fixing zone's claim on each node's reaction components
+    claim = np.stack([_zone_areas(bc, z)[:, None] * _fixed_axes(bc, z)[None, :]
+                      for z in fixing]) if fixing else np.zeros((0, bc.N, 3))
+    total = claim.sum(0)
+    share = np.divide(claim, total[None], out=np.zeros_like(claim), where=total[None] > 0)
+    forces = dict(zip(fixing, np.einsum("znk,nk->zk", share, reaction)))
     lumped = set(lumped)
     out = {}
     for zid, (f, S) in bc.sub.items():
-        ok = f >= 0
         kind = bc.bcs[zid]["kind"]
         if kind == "pressure":
-            p_sub = P[np.where(ok, f, 0)] if zid in lumped else bc.p_sub[zid]
-            out[zid] = (p_sub[..., None] * S * ok[..., None]).reshape(-1, 3).sum(0)
-            continue
-        share = np.divide(per[zid], tot, out=np.zeros_like(tot), where=tot > 0)
-        F = (share * react).sum(0)
-        if kind == "velocity" and not stokes:
-            F = F - np.einsum("fi,fik->k", bc.sub_flow[zid] * ok, bc.sub_vel[zid])
-        out[zid] = F
+            p = P[np.where(f >= 0, f, 0)] if zid in lumped else bc.p_sub[zid]
+            out[zid] = np.einsum("fi,fik->k", np.where(f >= 0, p, 0.0), S)
+        elif kind == "velocity" and not stokes:
+            out[zid] = forces[zid] - _inlet_momentum(bc, zid)
+        else:
+            out[zid] = forces[zid]
     return out
 
 
@@ -104,25 +115,19 @@ def wall_geometry(bc):
     """``(nodes, n, area, share)`` of the wall nodes (``zvcfd/fv/solver.py:1128-1161``): the
     nodes with wall sub-face area, their outward unit normals and wall areas, and the wall's
     fraction of the sub-face area of the zones fixing each node's velocity."""
-    N = bc.N
-    Sn, area = np.zeros((N, 3)), np.zeros(N)
-    wall, tot = np.zeros(N), np.zeros(N)
-    for zid, (f, S) in bc.sub.items():
-        kind = bc.bcs[zid]["kind"]
-        if kind not in ("wall", "velocity"):
-            continue
+    walls = [z for z in bc.sub if bc.bcs[z]["kind"] == "wall"]
+    inlets = [z for z in bc.sub if bc.bcs[z]["kind"] == "velocity"]
+    wall_area = sum((_zone_areas(bc, z) for z in walls), np.zeros(bc.N))
+    fixed_area = wall_area + sum((_zone_areas(bc, z) for z in inlets), np.zeros(bc.N))
+    outward = np.zeros((bc.N, 3))
+    for z in walls:
+        f, S = bc.sub[z]
         ok = f >= 0
-        a = np.bincount(f[ok], np.linalg.norm(S, axis=2)[ok], N)
-        tot += a
-        if kind == "wall":
-            wall += a
-            area += a
-            for k in range(3):
-                Sn[:, k] += np.bincount(f[ok], S[ok][:, k], N)
-    nodes = np.flatnonzero(area > 0)
-    n = Sn[nodes] / np.linalg.norm(Sn[nodes], axis=1, keepdims=True)
-    share = np.divide(wall, tot, out=np.zeros(N), where=tot > 0)[nodes]
-    return nodes, n, area[nodes], share
+        np.add.at(outward, f[ok], S[ok])
+    nodes = np.flatnonzero(wall_area > 0)
+    n = outward[nodes] / np.linalg.norm(outward[nodes], axis=1)[:, None]
+    share = wall_area[nodes] / fixed_area[nodes]
+    return nodes, n, wall_area[nodes], share
 
 
 def wall_shear_reaction(bc, residual: np.ndarray, P: np.ndarray, *, stokes: bool = False):
@@ -131,20 +136,18 @@ def wall_shear_reaction(bc, residual: np.ndarray, P: np.ndarray, *, stokes: bool
     each wall node, less the pressure force and the momentum of any inlet sub-faces the node
     also borders, over the node's wall area."""
     nodes, n, area, _ = wall_geometry(bc)
-    N = bc.N
-    F = -np.asarray(residual)[:, :3].copy()
+    F = -np.asarray(residual, float)[:, :3].copy()
     for zid, (f, S) in bc.sub.items():
         if bc.bcs[zid]["kind"] != "velocity":
             continue
         ok = f >= 0
-        for k in range(3):
-            F[:, k] -= np.bincount(f[ok], S[ok][:, k], N) * P
-            if not stokes:
-                mom = bc.sub_flow[zid] * bc.sub_vel[zid][..., k]
-                F[:, k] -= np.bincount(f[ok], mom[ok], N)
+        carried = S * P[np.where(ok, f, 0)][..., None]
+        if not stokes:
+            carried = carried + bc.sub_flow[zid][..., None] * bc.sub_vel[zid]
+        np.subtract.at(F, f[ok], carried[ok])
     F = F[nodes]
-    tau = F - np.einsum("nk,nk->n", F, n)[:, None] * n
-    return nodes, tau / area[:, None]
+    normal_part = np.einsum("nk,nk->n", F, n)
+    return nodes, (F - normal_part[:, None] * n) / area[:, None]
 
 
 __all__ = ["RawRows", "wall_geometry", "wall_shear_reaction", "zone_forces"]
