@@ -38,51 +38,47 @@ def block_weights(data, mode=0):
 
 
 def pairwise(n, indptr, indices, strength):
-    """Pairwise matching on coupling strength (``zvcfd/fv/linear.py:373-413``): four rounds of
-    mutual strongest free neighbours (ties: first in column order), pairs numbered in order
-    of their first node; unmatched nodes join their strongest aggregated neighbour, the rest
-    stay single. Returns ``(agg (n,), count)``."""
-    indptr = np.asarray(indptr, np.int64)
-    rows = np.repeat(np.arange(n), np.diff(indptr))
-    cols = np.asarray(indices, np.int64)
-    agg = -np.ones(n, np.int64)
-    off = rows != cols
-    r, c, s = rows[off], cols[off], strength[off]
-    nxt = 0
+    """Pairwise matching on coupling strength (``zvcfd/fv/linear.py:373-413``), node by node.
+
+    Up to four rounds: every free node picks its strongest free neighbour (the first in
+    column order among equals); nodes that pick each other form an aggregate, numbered in
+    order of the smaller node; the rounds stop early once no two free nodes are coupled.
+    Then every node still free joins the aggregate of its strongest already-aggregated
+    neighbour (picks made before any joins), and the rest become aggregates of their own, in
+    node order. Returns ``(agg (n,), count)``."""
+    ptr = [int(v) for v in indptr]
+    col = [int(v) for v in indices]
+    agg = [-1] * n
+    count = 0
+
+    def strongest(i, wanted):
+        pick, top = -1, None
+        for p in range(ptr[i], ptr[i + 1]):
+            j = col[p]
+            if j != i and wanted(j) and (top is None or strength[p] > top):
+                pick, top = j, strength[p]
+        return pick
+
     for _ in range(4):
-        m = (agg[r] < 0) & (agg[c] < 0)
-        if not m.any():
+        choice = {i: strongest(i, lambda j: agg[j] < 0) for i in range(n) if agg[i] < 0}
+        choice = {i: j for i, j in choice.items() if j >= 0}
+        if not choice:
             break
-        rr, cc, ss = r[m], c[m], s[m]
-        order = np.lexsort((-ss, rr))
-        rr, cc = rr[order], cc[order]
-        first = np.r_[True, rr[1:] != rr[:-1]]
-        best = -np.ones(n, np.int64)
-        best[rr[first]] = cc[first]
-        i = np.flatnonzero(best >= 0)
-        j = best[i]
-        mutual = (best[j] == i) & (i < j)
-        a, bb = i[mutual], j[mutual]
-        ids = nxt + np.arange(len(a))
-        agg[a] = ids
-        agg[bb] = ids
-        nxt += len(a)
-    left = np.flatnonzero(agg < 0)
-    if len(left):
-        m = (agg[r] < 0) & (agg[c] >= 0)
-        rr, cc, ss = r[m], c[m], s[m]
-        join = -np.ones(n, np.int64)
-        if len(rr):
-            order = np.lexsort((-ss, rr))
-            rr, cc = rr[order], cc[order]
-            first = np.r_[True, rr[1:] != rr[:-1]]
-            join[rr[first]] = agg[cc[first]]
-        to = join[left]
-        agg[left[to >= 0]] = to[to >= 0]
-        single = left[to < 0]
-        agg[single] = nxt + np.arange(len(single))
-        nxt += len(single)
-    return agg, nxt
+        for i in sorted(choice):
+            j = choice[i]
+            if i < j and choice.get(j) == i:
+                agg[i] = agg[j] = count
+                count += 1
+    free = [i for i in range(n) if agg[i] < 0]
+    joins = {i: strongest(i, lambda j: agg[j] >= 0) for i in free}
+    for i in free:
+        if joins[i] >= 0:
+            agg[i] = agg[joins[i]]
+    for i in free:
+        if joins[i] < 0:
+            agg[i] = count
+            count += 1
+    return np.array(agg, np.int64), count
 
 
 def transpose_positions(indptr, indices):
@@ -203,6 +199,13 @@ class ACM:
         return self._smooth(L, x, b, self.smooth)
 
 
+def givens(a, b):
+    """The 2x2 rotation that takes ``(a, b)`` to ``(hypot(a, b), 0)``."""
+    r = np.hypot(a, b)
+    c, s = (a / r, b / r) if r else (1.0, 0.0)
+    return np.array([[c, s], [-s, c]])
+
+
 def fgmres(matvec, b, x0, precond, *, rtol=1e-6, restart=30, maxiter=300):
     """Right-preconditioned flexible GMRES with CGS2 (``zvcfd/fv/linear.py:172-320``):
     convergence relative to the initial residual, with the round-off floor 1e-13 ||b||.
@@ -220,7 +223,7 @@ def fgmres(matvec, b, x0, precond, *, rtol=1e-6, restart=30, maxiter=300):
         H = np.zeros((restart + 1, restart))
         g = np.zeros(restart + 1)
         g[0] = beta
-        cs, sn = np.zeros(restart), np.zeros(restart)
+        rot = [None] * restart
         kk = 0
         for k in range(restart):
             z = precond(V[k])
@@ -234,15 +237,11 @@ def fgmres(matvec, b, x0, precond, *, rtol=1e-6, restart=30, maxiter=300):
             hn = np.linalg.norm(w)
             H[:k + 1, k] = h1 + h2
             H[k + 1, k] = hn
-            for j in range(k):
-                t = cs[j] * H[j, k] + sn[j] * H[j + 1, k]
-                H[j + 1, k] = -sn[j] * H[j, k] + cs[j] * H[j + 1, k]
-                H[j, k] = t
-            den = np.hypot(H[k, k], H[k + 1, k])
-            cs[k], sn[k] = (H[k, k] / den, H[k + 1, k] / den) if den else (1.0, 0.0)
-            H[k, k], H[k + 1, k] = den, 0.0
-            g[k + 1] = -sn[k] * g[k]
-            g[k] = cs[k] * g[k]
+            for j in range(k):                    # the earlier plane rotations
+                H[j:j + 2, k] = rot[j] @ H[j:j + 2, k]
+            rot[k] = givens(H[k, k], H[k + 1, k])
+            H[k:k + 2, k] = rot[k] @ H[k:k + 2, k]
+            g[k:k + 2] = rot[k] @ g[k:k + 2]
             it += 1
             kk = k + 1
             res = abs(g[k + 1]) / bnorm

@@ -155,3 +155,30 @@ def test_symmetrised_strength_keeps_pairwise_coarsening_under_convection():
     _, symmetric = aggregate(ip, cols, data, 2, 2)
     assert one_sided > 0.5 * n
     assert symmetric < 0.25 * n
+
+
+def test_oracle_acm_fgmres_solves_an_assembled_system():
+    """The oracle's linear solver (the reference ACM's V-cycle inside FGMRES) on a Dirichlet
+    system the oracle assembled for a golden pipe reaches the direct solution."""
+    import scipy.sparse.linalg as spl
+
+    from fixtures import fluid_of, mesh_of, pipe_bcs
+    from oracle.fv import OracleSolver
+    from oracle.linear import ACM, fgmres
+
+    g = load("pipe_tet_si")
+    m = mesh_of(g)
+    s = OracleSolver(m, fluid_of(g), pipe_bcs("pipe_tet_si", g, m), advection=1.0)
+    s.solve(max_iterations=3, tol=0.0)
+    data, b = s.assemble()
+    A = s.to_csr(data)
+    amg = ACM().setup(s.indptr, s.indices, data)
+    assert len(amg.levels) >= 2
+    x, its, res, ok = fgmres(lambda v: A @ v, b.reshape(-1), np.zeros(b.size), amg.vcycle,
+                             rtol=1e-10, maxiter=300)
+    assert ok and res <= 1e-10 * 1.01
+    assert np.linalg.norm(A @ x - b.reshape(-1)) <= 1.01e-10 * np.linalg.norm(b)
+    # the system's condition number is about 7e7: the fields agree to that times the residual
+    X, R = x.reshape(-1, 4), spl.spsolve(A.tocsc(), b.reshape(-1)).reshape(-1, 4)
+    assert np.abs(X[:, :3] - R[:, :3]).max() < 1e-5 * np.abs(R[:, :3]).max()
+    assert np.abs(X[:, 3] - R[:, 3]).max() < 1e-5 * np.ptp(R[:, 3])
