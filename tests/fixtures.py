@@ -81,41 +81,44 @@ def oracle_kernel_outputs(g: dict) -> dict:
             "dnode": dnode, "snode": snode, "solver": s}
 
 
-def pipe_bcs(name: str, g: dict, m):
-    """The boundary conditions the golden pipe case was solved with."""
+def axial_parabola(radius: float, peak: float = 1.0, pulse=None):
+    """``u(x)`` (or ``u(x, t)`` with ``pulse(t)``): velocity along +z, ``peak (1 - r^2/R^2)``
+    inside the radius and zero outside, ``r`` the distance from the z axis."""
+    def shape(x):
+        r2 = np.einsum("ij,ij->i", x[:, :2], x[:, :2]) / radius ** 2
+        u = np.zeros((len(x), 3))
+        u[:, 2] = peak * np.maximum(1.0 - r2, 0.0)
+        return u
+
+    if pulse is None:
+        return shape
+    return lambda x, t: pulse(t) * shape(x)
+
+
+def _pipe_zones(m, inlet: dict) -> dict:
     z = {zz.name: k for k, zz in m.zones.items()}
-    if name == "pipe_reference_tube" or name == "pipe_tet_si":
-        R, umax = float(g["radius"]), float(g["umax"])
-
-        def prof(x):
-            r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
-            return np.stack([0 * r2, 0 * r2, umax * np.clip(1 - r2, 0, None)], 1)
-
-        inlet = {"kind": "velocity", "value": prof}
-    else:
-        def shape(x):
-            r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / (2e-3) ** 2
-            return np.clip(1 - r2, 0, None)
-
-        inlet = {"kind": "velocity", "flow_rate": float(g["flow_rate"]), "profile": shape}
     return {z["inlet"]: inlet, z["outlet"]: {"kind": "pressure", "value": 0.0},
             z["wall"]: {"kind": "wall"}}
+
+
+def pipe_bcs(name: str, g: dict, m):
+    """The boundary conditions the golden pipe case was solved with."""
+    if name in ("pipe_reference_tube", "pipe_tet_si"):
+        inlet = {"kind": "velocity", "value": axial_parabola(float(g["radius"]), float(g["umax"]))}
+    else:
+        profile = axial_parabola(2e-3)
+        inlet = {"kind": "velocity", "flow_rate": float(g["flow_rate"]),
+                 "profile": lambda x: profile(x)[:, 2]}
+    return _pipe_zones(m, inlet)
 
 
 PIPES = ("pipe_reference_tube", "pipe_tet_si", "curved_cy")
 
 
 def transient_bcs(g: dict, m):
-    R, umax = float(g["radius"]), float(g["umax"])
-    z = {zz.name: k for k, zz in m.zones.items()}
-
-    def prof(x, t):
-        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
-        amp = 1.0 + 0.5 * np.sin(2 * np.pi * t / 0.8)
-        return np.stack([0 * r2, 0 * r2, umax * amp * np.clip(1 - r2, 0, None)], 1)
-
-    return {z["inlet"]: {"kind": "velocity", "value": prof},
-            z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    pulse = axial_parabola(float(g["radius"]), float(g["umax"]),
+                           pulse=lambda t: 1.0 + 0.5 * np.sin(2 * np.pi * t / 0.8))
+    return _pipe_zones(m, {"kind": "velocity", "value": pulse})
 
 
 def backflow_bcs(m, beta: float) -> dict:
@@ -136,14 +139,7 @@ def forces_case(g: dict, tag: str):
     m = mesh_of(sub)
     z = {zz.name: k for k, zz in m.zones.items()}
     if tag == "pipe":
-        R = 0.5
-
-        def prof(x):
-            r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
-            return np.stack([0 * r2, 0 * r2, 2 * np.clip(1 - r2, 0, None)], 1)
-
-        bcs = {z["inlet"]: {"kind": "velocity", "value": prof},
-               z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+        bcs = _pipe_zones(m, {"kind": "velocity", "value": axial_parabola(0.5, 2.0)})
     else:
         bcs = {z["xmin"]: {"kind": "velocity", "value": [1.0, 0.0, 0.0]},
                z["xmax"]: {"kind": "pressure", "value": 0.0},

@@ -84,51 +84,61 @@ def blocks_on_pattern(M, indptr, indices) -> np.ndarray:
     return data
 
 
-def kernel_case(name: str, gn: bool, dt) -> dict:
+# the random-state kernel test of the reference (tests/test_fv_fast.py:98-159): its fluid,
+# viscosity law and seed, so that the vectors are those its own check compares
+KERNEL_RHO, KERNEL_MU, KERNEL_SEED = 1.3, 0.7, 11
+KERNEL_CY = dict(mu_0=0.9, mu_inf=0.1, lam=1.5)
+
+
+def _without_time_terms(s, dt):
+    """The reference's raw rows less its time diagonal ``rho V / dt`` on the momentum rows
+    (and the matching right-hand side), which the device assembly adds later."""
     import scipy.sparse as sp
 
+    M, b = s._raw
+    if not dt:
+        return M, b
+    mass = KERNEL_RHO * s.V / dt
+    M = M - sp.diags(np.kron(mass, [1.0, 1.0, 1.0, 0.0]))
+    b = b - np.hstack([mass[:, None] * s.U, np.zeros((s.N, 1))]).ravel()
+    return M, b
+
+
+def kernel_case(name: str, gn: bool, dt) -> dict:
     m = MESHES[name]()
-    rho, mu = 1.3, 0.7
-    cy = CarreauYasuda(mu_0=0.9, mu_inf=0.1, lam=1.5)
-    fl = Fluid(rho, mu, viscosity=cy if gn else None)
-    s = ReferenceSolver(m, fl, {z: {"kind": "wall"} for z in m.zones},
+    cy = CarreauYasuda(**KERNEL_CY)
+    s = ReferenceSolver(m, Fluid(KERNEL_RHO, KERNEL_MU, viscosity=cy if gn else None),
+                        {zid: {"kind": "wall"} for zid in m.zones},
                         advection="high-resolution", lag_rhie_chow=True, dt=dt, transpose=gn)
-    rng = np.random.default_rng(11)
-    s.U = rng.normal(size=(s.N, 3))
-    s.P = rng.normal(size=s.N)
+    draw = np.random.default_rng(KERNEL_SEED)
+    # a random state, drawn in this order: velocity, pressure, mass flows per kind, blend
+    state = {"U": draw.normal(size=(s.N, 3)), "P": draw.normal(size=s.N)}
+    mdot = {}
     for K in s.kinds:
-        K.mdot = rng.normal(size=K.mdot.shape)
-    s._frozen_beta = rng.uniform(0, 1, (s.N, 3))
-    U0, P0 = s.U.copy(), s.P.copy()
-    mdot0 = {K.kind: K.mdot.copy() for K in s.kinds}
-    beta0 = s._frozen_beta.copy()
+        K.mdot = mdot[K.kind] = draw.normal(size=K.mdot.shape)
+    state["beta_frozen"] = draw.uniform(0, 1, (s.N, 3))
+    s.U, s.P, s._frozen_beta = state["U"].copy(), state["P"].copy(), state["beta_frozen"].copy()
+    mdot = {k: v.copy() for k, v in mdot.items()}
     s._store_old(first=True)
     s.assemble()
-    M_raw, b_raw = s._raw
-    if dt:
-        t = rho * s.V / dt
-        M_raw = M_raw - sp.diags(np.repeat(t, 4) * np.tile([1, 1, 1, 0], s.N))
-        b_raw = b_raw - np.column_stack([t[:, None] * s.U, np.zeros(s.N)]).reshape(-1)
+    M_raw, b_raw = _without_time_terms(s, dt)
     indptr, indices = node_graph(m)
-    gradU, gradP = s.nodal_gradient(U0), s.nodal_gradient(P0)
-    out = mesh_arrays(m)
+    gradU, gradP = s.nodal_gradient(state["U"]), s.nodal_gradient(state["P"])
+    out = dict(mesh_arrays(m), **state)
     out.update({
-        "rho": rho, "mu": mu, "gn": int(gn), "dt": 0.0 if dt is None else dt,
+        "rho": KERNEL_RHO, "mu": KERNEL_MU, "gn": int(gn), "dt": 0.0 if dt is None else dt,
         "cy": np.array([cy.mu_0, cy.mu_inf, cy.lam, cy.a, cy.n]),
-        "U": U0, "P": P0, "beta_frozen": beta0,
         "V": s.V, "gradU": gradU, "gradP": gradP, "diag": s._a_space,
         "beta_limiter": s._beta(gradU), "indptr": indptr, "indices": indices,
         "data_raw": blocks_on_pattern(M_raw, indptr, indices), "b_raw": b_raw.reshape(-1, 4),
     })
-    for k, v in mdot0.items():
-        out[f"mdot_{k}"] = v
-    # mass flows of a new state with the previous one as the old level
-    U_new, P_new = rng.normal(size=(s.N, 3)), rng.normal(size=s.N)
-    s.U, s.P = U_new, P_new
+    out.update({f"mdot_{k}": v for k, v in mdot.items()})
+    # mass flows of a new random state, the drawn one being the old level
+    s.U, s.P = draw.normal(size=(s.N, 3)), draw.normal(size=s.N)
+    out.update({"U_new": s.U.copy(), "P_new": s.P.copy()})
     s.update_mass_flows()
-    out.update({"U_new": U_new, "P_new": P_new, "imbalance": s._interior_out})
-    for K in s.kinds:
-        out[f"mdot_new_{K.kind}"] = K.mdot
+    out["imbalance"] = s._interior_out
+    out.update({f"mdot_new_{K.kind}": K.mdot for K in s.kinds})
     return out
 
 
@@ -467,6 +477,13 @@ def lumped_case() -> dict:
 
 
 def main():
+    if sys.argv[1:] == ["kernels"]:
+        for name in MESHES:
+            for gn, dt in VARIANTS:
+                tag = f"kernel_{name}_{'gn' if gn else 'newt'}_{'dt' if dt else 'steady'}"
+                np.savez_compressed(HERE / f"{tag}.npz", **kernel_case(name, gn, dt))
+        print("wrote kernels")
+        return
     if sys.argv[1:] == ["profiles"]:
         np.savez_compressed(HERE / "profiles.npz", **profiles_case())
         print("wrote profiles")
