@@ -58,3 +58,31 @@ def test_ensemble_vessels_are_sized_and_seeded(kind, nodes):
     again, _, _ = vessel(kind, nodes, 5)
     np.testing.assert_array_equal(m.nodes, again.nodes)
     assert all(o in {z.name for z in m.zones.values()} for o in outlets)
+
+
+@pytest.mark.parametrize("name", ["pipe_reference_tube", "curved_cy"])
+def test_wall_operator_gives_the_reference_wall_shear(name):
+    """The device wall-shear operator's host data (owning elements, shape gradients at the
+    wall integration points, normals, areas), applied here with NumPy the way the kernel
+    applies it, reproduces the reference's wall shear on the converged golden fields."""
+    from fixtures import fluid_of, load, mesh_of
+    from zvcfd_b200.wall import wall_operator
+
+    g = load(name)
+    m = mesh_of(g)
+    fl = fluid_of(g)
+    walls = [z for z, zz in m.zones.items() if zz.name == "wall"]
+    elem, G, nrm, area, node = wall_operator(m, walls)
+    U = g["U"]
+    grad = np.einsum("qar,qac->qrc", np.where(elem[..., None] >= 0, U[np.maximum(elem, 0)], 0.0), G)
+    D = grad + np.swapaxes(grad, 1, 2)
+    mu = np.full(len(D), fl.mu) if fl.viscosity is None else \
+        fl.viscosity(np.sqrt(0.5 * np.einsum("qrc,qrc->q", D, D)))
+    t = mu[:, None] * np.einsum("qrc,qc->qr", D, nrm)
+    sub = -(t - np.einsum("qr,qr->q", t, nrm)[:, None] * nrm)
+    tau = np.zeros((m.n_nodes, 3))
+    np.add.at(tau, node, sub * area[:, None])
+    weight = np.bincount(node, area, m.n_nodes)
+    tau[weight > 0] /= weight[weight > 0, None]
+    ref = load("wall_shear")[f"{name}_tau"]
+    np.testing.assert_allclose(tau, ref, atol=1e-12 * np.abs(ref).max())

@@ -22,68 +22,87 @@ from zvcfd_b200.topology import FACES, REF_NODES, _parameters_of, shape_function
 MAXN = 8
 
 
+def _face_keys(faces: np.ndarray, n_nodes: int):
+    """Two int64 keys per face from its sorted node ids (``-1`` pads count as 0): equal keys,
+    equal faces."""
+    k = np.sort(faces, axis=1) + 1
+    base = np.int64(n_nodes + 1)
+    return k[:, 0] * base + k[:, 1], k[:, 2] * base + k[:, 3]
+
+
 def face_owners(mesh, faces: np.ndarray):
-    """``(kind per face, element row)`` of the element owning each boundary face."""
-    keys, kinds, rows = [], [], []
+    """``(kind per face, element row)`` of the element owning each boundary face: the element
+    faces and the queried faces are sorted together by key, and each queried face takes the
+    element face next to it in that order when their keys agree."""
+    owner_kind, owner_row, el_faces = [], [], []
     for kind, e in mesh.elements.items():
-        for fl in FACES[kind]:
-            loc = e[:, list(fl)]
-            if len(fl) == 3:
-                loc = np.concatenate([loc, -np.ones((len(e), 1), np.int64)], 1)
-            keys.append(np.sort(loc, 1))
-            kinds.append(np.full(len(e), kind, dtype=object))
-            rows.append(np.arange(len(e)))
-    keys, kinds, rows = np.concatenate(keys), np.concatenate(kinds), np.concatenate(rows)
-    fk = np.sort(faces, 1)
-    allk = np.concatenate([keys, fk])
-    _, inv = np.unique(allk, axis=0, return_inverse=True)
-    inv = inv.reshape(-1)
-    where = -np.ones(inv.max() + 1, np.int64)
-    where[inv[:len(keys)]] = np.arange(len(keys))
-    hit = where[inv[len(keys):]]
+        for local in FACES[kind]:
+            pad = np.full((len(e), 4 - len(local)), -1, np.int64)
+            el_faces.append(np.concatenate([e[:, list(local)], pad], 1))
+            owner_kind.append(np.full(len(e), kind, dtype=object))
+            owner_row.append(np.arange(len(e)))
+    el_faces = np.concatenate(el_faces)
+    owner_kind, owner_row = np.concatenate(owner_kind), np.concatenate(owner_row)
+    hi, lo = _face_keys(np.concatenate([el_faces, faces]), mesh.n_nodes)
+    is_query = np.r_[np.zeros(len(el_faces), bool), np.ones(len(faces), bool)]
+    # element faces sort before the queried copy of the same face
+    order = np.lexsort((is_query, lo, hi))
+    hit = np.full(len(faces), -1, np.int64)
+    q = np.flatnonzero(is_query[order][1:]) + 1           # positions of queried faces
+    prev = order[q - 1]
+    same = (hi[prev] == hi[order[q]]) & (lo[prev] == lo[order[q]]) & ~is_query[prev]
+    hit[order[q][same] - len(el_faces)] = prev[same]
     if (hit < 0).any():
         raise ValueError(f"{int((hit < 0).sum())} wall faces belong to no element")
-    return kinds[hit], rows[hit]
+    return owner_kind[hit], owner_row[hit]
+
+
+def _local_positions(e: np.ndarray, f: np.ndarray, n_nodes: int) -> np.ndarray:
+    """``(F, 4)``: where each node of face ``f[i]`` sits in element ``e[i]`` (0 for pads),
+    found by a search in each element's sorted node list."""
+    shift = (np.arange(len(e), dtype=np.int64) * (n_nodes + 1))[:, None]
+    order = np.argsort(e, axis=1)
+    flat = (np.take_along_axis(e, order, 1) + shift).ravel()
+    at = np.searchsorted(flat, (np.where(f >= 0, f, e[:, :1]) + shift).ravel())
+    at = at.reshape(f.shape) - np.arange(len(e))[:, None] * e.shape[1]
+    return np.where(f >= 0, np.take_along_axis(order, at, 1), 0)
 
 
 def wall_operator(mesh, zone_ids):
     """Per wall sub-face integration point: owning element's nodes ``(M, 8)`` (-1 padded),
-    shape-function gradients ``(M, 8, 3)``, unit outward normal, area and wall node."""
+    shape-function gradients ``(M, 8, 3)``, unit outward normal, area and wall node.
+
+    The integration point of a sub-face is its area centroid; in the owning element's
+    reference coordinates that is the same weights applied to the face nodes' reference
+    positions, where the element's shape functions give ``grad N = J^-T dN``."""
     faces = np.concatenate([mesh.zones[z].faces for z in zone_ids])
     kind_of, erow = face_owners(mesh, faces)
     W = subface_weights(faces)
     S = subfaces(mesh.nodes, faces)
-    elem, G, nrm, area, node = [], [], [], [], []
+    parts = []
     for kind in mesh.elements:
         fsel = np.flatnonzero(kind_of == kind)
         if not len(fsel):
             continue
         e = mesh.elements[kind][erow[fsel]]
         f = faces[fsel]
-        ok = f >= 0
-        loc = np.argmax(e[:, None, :] == np.where(ok, f, -2)[:, :, None], axis=2)
-        ref = np.asarray(REF_NODES[kind], float)[loc]
-        ref = np.where(ok[..., None], ref, 0.0)
-        pts = np.einsum("fij,fjd->fid", W[fsel], ref)
-        fi, si = np.nonzero(ok)
-        _, dN = shape_functions(kind, _parameters_of(kind, pts[fi, si]))
+        ref = np.asarray(REF_NODES[kind], float)[_local_positions(e, f, mesh.n_nodes)]
+        ref[f < 0] = 0.0
+        ips = np.einsum("fij,fjd->fid", W[fsel], ref)
+        fi, si = np.nonzero(f >= 0)
+        _, dN = shape_functions(kind, _parameters_of(kind, ips[fi, si]))    # (M, n, 3)
         x = mesh.nodes[e[fi]]
-        J = np.einsum("mnk,mnd->mkd", x, dN)
-        g = np.einsum("mnd,mdk->mnk", dN, np.linalg.inv(J))
-        a = S[fsel][fi, si]
-        ar = np.linalg.norm(a, axis=1)
+        J = np.einsum("mnk,mnd->mkd", x, dN)                                # dx_k / dxi_d
+        grad = np.swapaxes(np.linalg.solve(np.swapaxes(J, 1, 2), np.swapaxes(dN, 1, 2)), 1, 2)
+        vec = S[fsel][fi, si]
+        size = np.linalg.norm(vec, axis=1)
         n = e.shape[1]
-        ep = -np.ones((len(fi), MAXN), np.int64)
-        ep[:, :n] = e[fi]
-        gp = np.zeros((len(fi), MAXN, 3))
-        gp[:, :n] = g
-        elem.append(ep)
-        G.append(gp)
-        nrm.append(a / ar[:, None])
-        area.append(ar)
-        node.append(f[fi, si])
-    return (np.concatenate(elem), np.concatenate(G), np.concatenate(nrm), np.concatenate(area),
-            np.concatenate(node))
+        elem = np.full((len(fi), MAXN), -1, np.int64)
+        elem[:, :n] = e[fi]
+        G = np.zeros((len(fi), MAXN, 3))
+        G[:, :n] = grad
+        parts.append((elem, G, vec / size[:, None], size, f[fi, si]))
+    return tuple(np.concatenate(col) for col in zip(*parts))
 
 
 class WallShear:
