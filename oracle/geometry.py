@@ -15,40 +15,47 @@ def element_points(x: np.ndarray, kind: str) -> np.ndarray:
     return np.einsum("pn,enk->epk", tables(kind).weights, x)
 
 
+def _flux_triangles(P: np.ndarray, kind: str):
+    """The three corners ``(E, n_ip, 3)`` each of every flux point's dual-face triangle."""
+    T = P[:, tables(kind).tris]
+    return T[:, :, 0], T[:, :, 1], T[:, :, 2]
+
+
 def ip_areas(P: np.ndarray, kind: str) -> np.ndarray:
     """Flux-point area vectors ``(E, n_ip, 3)``, edge node a -> b (``geometry.py:182-185``)."""
-    T = P[:, tables(kind).tris]
-    return 0.5 * np.cross(T[:, :, 1] - T[:, :, 0], T[:, :, 2] - T[:, :, 0])
+    p0, p1, p2 = _flux_triangles(P, kind)
+    return 0.5 * np.cross(p1 - p0, p2 - p0)
 
 
 def ip_points(P: np.ndarray, kind: str) -> np.ndarray:
     """Flux-point centroids ``(E, n_ip, 3)`` (``geometry.py:188-190``)."""
-    return P[:, tables(kind).tris].mean(2)
+    p0, p1, p2 = _flux_triangles(P, kind)
+    return (p0 + p1 + p2) / 3.0
 
 
 def scv_volumes(P: np.ndarray, kind: str) -> np.ndarray:
-    """Sub-control volumes ``(E, n)`` by the divergence theorem (``geometry.py:193-215``)."""
+    """Sub-control volumes ``(E, n)`` by the divergence theorem (``geometry.py:193-215``): the
+    volume of a node's part of the element is a third of the flux of ``x - x_node`` out of it,
+    and only the dual faces (the flux-point triangles) carry any, the rest of its boundary
+    lying in element faces through the node."""
     t = tables(kind)
-    T = P[:, t.tris]
-    A = 0.5 * np.cross(T[:, :, 1] - T[:, :, 0], T[:, :, 2] - T[:, :, 0])
-    cen = T.mean(2)
+    A, c = ip_areas(P, kind), ip_points(P, kind)
     x = P[:, :t.n]
-    a, b = t.edge[:, 0], t.edge[:, 1]
-    ca = np.einsum("eik,eik->ei", cen - x[:, a], A)
-    cb = -np.einsum("eik,eik->ei", cen - x[:, b], A)
-    Ma = np.zeros((t.n_ip, t.n))
-    Mb = np.zeros((t.n_ip, t.n))
-    Ma[np.arange(t.n_ip), a] = 1.0
-    Mb[np.arange(t.n_ip), b] = 1.0
-    return (ca @ Ma + cb @ Mb) / 3.0
+    vol = np.zeros((len(P), t.n))
+    for s, (a, b) in enumerate(t.edge):          # the area points from node a to node b
+        vol[:, a] += np.einsum("ek,ek->e", c[:, s] - x[:, a], A[:, s]) / 3.0
+        vol[:, b] -= np.einsum("ek,ek->e", c[:, s] - x[:, b], A[:, s]) / 3.0
+    return vol
 
 
 def gradients(x: np.ndarray, kind: str) -> np.ndarray:
-    """Shape-function gradients at the flux points ``(E, n_ip, n, 3)`` (``geometry.py:218-223``)."""
-    t = tables(kind)
-    J = np.einsum("enk,ind->eikd", x, t.dN_ip)
-    Jinv = np.linalg.inv(J)
-    return np.einsum("ind,eidk->eink", t.dN_ip, Jinv)
+    """Shape-function gradients at the flux points ``(E, n_ip, n, 3)`` (``geometry.py:218-223``):
+    ``grad N = J^-T dN``, ``J`` the Jacobian of the element map there."""
+    dN = tables(kind).dN_ip                                  # (n_ip, n, 3)
+    J = np.einsum("enk,ind->eikd", x, dN)                    # dx_k / dxi_d
+    Jt = np.swapaxes(J, -1, -2)
+    rhs = np.broadcast_to(np.swapaxes(dN, -1, -2)[None], Jt.shape[:2] + (3, dN.shape[1]))
+    return np.swapaxes(np.linalg.solve(Jt, rhs), -1, -2)
 
 
 def boundary_subfaces(nodes: np.ndarray, faces: np.ndarray) -> np.ndarray:

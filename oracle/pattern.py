@@ -22,18 +22,21 @@ _M64 = (1 << 64) - 1
 
 
 def node_graph(mesh):
-    """``(indptr int64 (N+1,), indices int64)`` of node couplings (``pattern.py:18-33``)."""
-    N = mesh.n_nodes
-    keys = []
+    """``(indptr int64 (N+1,), indices int64)`` of node couplings (``pattern.py:18-33``): every
+    ordered pair of nodes of every element, itself included, sorted and counted once."""
+    rows, cols = [], []
     for e in mesh.elements.values():
         n = e.shape[1]
-        ii, jj = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
-        keys.append(np.unique(e[:, ii.ravel()] * N + e[:, jj.ravel()]))
-    key = np.unique(np.concatenate(keys))
-    rows = key // N
-    indptr = np.zeros(N + 1, np.int64)
-    np.cumsum(np.bincount(rows, minlength=N), out=indptr[1:])
-    return indptr, (key % N).astype(np.int64)
+        rows.append(np.repeat(e, n, axis=1).ravel())
+        cols.append(np.tile(e, (1, n)).ravel())
+    r, c = np.concatenate(rows), np.concatenate(cols)
+    order = np.lexsort((c, r))
+    r, c = r[order], c[order]
+    first = np.r_[True, (r[1:] != r[:-1]) | (c[1:] != c[:-1])]
+    r, c = r[first], c[first]
+    indptr = np.zeros(mesh.n_nodes + 1, np.int64)
+    indptr[1:] = np.cumsum(np.bincount(r, minlength=mesh.n_nodes))
+    return indptr, c.astype(np.int64)
 
 
 def element_keys(E: int) -> np.ndarray:
