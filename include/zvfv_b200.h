@@ -186,7 +186,7 @@ int zvfv_update_noalloc(int64_t n, const double *x, double *U, double *P, double
                         void *stream);
 
 /* Wall shear stress (N, 3) at wall nodes from the wall integration points of their sub-faces
- * (WallGradientShear.__call__, zvcfd/fv/wall.py:107-137): node_ptr int64 (N+1) groups the
+ * (WallGradientShear.__call__, zvcfd/fv/wall.py:113-137): node_ptr int64 (N+1) groups the
  * ips by node; per ip the owning element's nodes elem int32 (M, 8, -1 padded), shape
  * gradients grad (M, 8, 3), unit outward normal (M, 3) and area (M). */
 int zvfv_wall_shear(int64_t n_nodes, const int64_t *node_ptr, const int32_t *elem,
@@ -205,13 +205,13 @@ int zvfv_bsr_residual(int64_t n, const int64_t *indptr, const int32_t *indices,
                       const double *data, const double *x, const double *b, double *r, int lanes,
                       void *stream);
 /* y = A x with FP32 blocks and vectors (the mixed-precision hierarchy's product; AmgX mode
- * dDFI's matrix precision, zvcfd/fv/linear.py:525, :854-855) */
+ * dDFI's matrix precision, zvcfd/fv/linear.py:523-524, :853-854) */
 int zvfv_bsr_spmv_f32(int64_t n, const int64_t *indptr, const int32_t *indices,
                       const float *data, const float *x, float *y, int lanes, void *stream);
 
 /* The structure of A^T (built once per pattern): tptr int64 (n+1), per entry the row trow
  * int32 (ascending within a column) and the block index tperm int64 of A. Replaces the
- * reference's host transposes (BlockMatrix.to_scipy().T, zvcfd/fv/linear.py:115-135). */
+ * reference's host transposes (BlockMatrix.to_scipy().T, zvcfd/fv/linear.py:123-135). */
 int zvfv_bsr_transpose(int64_t n, int64_t nnz, const int64_t *indptr, const int32_t *indices,
                        int64_t *tptr, int32_t *trow, int64_t *tperm, void *stream);
 /* y = A^T x (the discrete adjoint's product; lanes 8, 16 or 32) */
@@ -224,7 +224,7 @@ int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const i
  * API the reference binds (AMGX_config_create / resources / matrix / solver handles,
  * zvcfd/fv/linear.py:728-739, :846-868, :905-955) and its own ACM (linear.py:328-518).
  * create: precision 0 FP64, 1 FP32 hierarchy; smoother 0 damped block Jacobi, 1 symmetric
- * multicolour block Gauss-Seidel (AmgX's MULTICOLOR_GS of the `gs` preset, linear.py:76-79);
+ * multicolour block Gauss-Seidel (AmgX's MULTICOLOR_GS of the `gs` preset, linear.py:571-598);
  * strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
  * directions of each coupling (the default of the Python back end: convection otherwise
  * stalls the pairwise matching). rebuild_every > 0 re-aggregates every that many
@@ -236,12 +236,12 @@ int zvfv_solver_create(void **handle, int precision, int smoother, int strength,
                        int presweeps, int postsweeps, double omega, int coarse_sweeps,
                        int max_levels, int rebuild_every, int restart);
 /* structure on the first call (or when it changes), coefficients after: AMGX_matrix_upload_all
- * / AMGX_matrix_replace_coefficients + AMGX_solver_setup (zvcfd/fv/linear.py:327-349, :310) */
+ * / AMGX_matrix_replace_coefficients + AMGX_solver_setup (zvcfd/fv/linear.py:846-868, :812-840) */
 int zvfv_solver_setup(void *handle, int64_t n, int64_t nnzb, const int64_t *indptr,
                       const int32_t *indices, const double *data, void *stream);
 /* x (in: x0, out: solution) to a reduction rtol of the initial residual, with n_lowrank
  * rank-one terms u w^T (BlockMatrix.lowrank, zvcfd/fv/linear.py:81-103): AMGX_solver_solve
- * (linear.py:401-436) / fgmres (linear.py:172-320). Synchronises once per Krylov step. */
+ * (linear.py:920-955) / fgmres (linear.py:172-320). Synchronises once per Krylov step. */
 int zvfv_solver_solve(void *handle, const double *b, double *x, double rtol, int maxiter,
                       int n_lowrank, const int64_t *const *u_idx, const double *const *u_val,
                       const int64_t *u_len, const int64_t *const *w_idx, const double *const *w_val,
@@ -255,7 +255,7 @@ int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, i
                         const int64_t *u_len, const int64_t *const *w_idx,
                         const double *const *w_val, const int64_t *w_len, int *iterations,
                         double *residual, int *converged, void *stream);
-/* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:386-399) */
+/* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:905-918) */
 int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
 /* Hierarchy options beyond create (each takes effect at the next set-up, which rebuilds):
  *   "autotune" (0/1, default 0): after each rebuild, every level of 2048 rows or more times one
@@ -269,12 +269,12 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
 int zvfv_solver_set_option(void *handle, const char *name, double value);
 /* The value of an option above, or a counter: "rebuilds" (hierarchy builds so far), "setups". */
 int zvfv_solver_get_option(void *handle, const char *name, double *value);
-/* hierarchy sizes (ACM.stats, zvcfd/fv/linear.py:513-518) */
+/* hierarchy sizes (ACM.stats, zvcfd/fv/linear.py:515-518) */
 int zvfv_solver_stats(void *handle, int max_levels, int *levels, int64_t *rows, int64_t *blocks);
 /* one level's size and aggregates (agg: n int32 entries, or NULL) */
 int zvfv_solver_level(void *handle, int level, int64_t *n, int64_t *nnzb, int64_t *n_coarse,
                       int32_t *agg, void *stream);
-/* AMGX_solver_destroy / matrix / vector / resources (zvcfd/fv/linear.py:351-384) */
+/* AMGX_solver_destroy / matrix / vector / resources (AMGX.close, zvcfd/fv/linear.py:870-903) */
 int zvfv_solver_destroy(void *handle);
 
 #ifdef __cplusplus
