@@ -142,3 +142,26 @@ def test_raw_rows_residual_on_a_random_state():
             - b.reshape(-1)).reshape(-1, 4)
     np.testing.assert_allclose(r[keep], full[keep], atol=1e-12 * np.abs(full).max())
     assert raw.nraw == int(np.sum((s.indptr[1:] - s.indptr[:-1])[keep]))
+
+
+@pytest.mark.parametrize("tag", ["pipe", "channel"])
+def test_solver_zone_forces_glue_on_cpu_tensors(tag):
+    """``B200Solver.zone_forces`` and ``wall_shear("reaction")`` over the buffers the boundary
+    pass fills (here from the oracle, as CPU tensors): the solver's own glue, without a GPU."""
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.solver import B200Solver
+
+    m, bcs, sub, s = _solved(tag)
+    bc = Boundary(m, bcs, 1.0)
+    ip, ix, rawoff, rawdata, rawb = _compact(s, bc.vel_fixed_comp.any(1))
+    sv = object.__new__(B200Solver)
+    sv.pattern, sv._rawoff, sv.rawdata, sv.rawb = (ip, ix), rawoff, rawdata, rawb.reshape(-1)
+    sv.U, sv.P = torch.as_tensor(s.U), torch.as_tensor(s.P)
+    sv.bc, sv.stokes, sv._lumped, sv._assembled, sv._raw_rows = bc, False, {}, True, None
+    F = sv.zone_forces()
+    got = np.array([F[int(z)] for z in sub["force_zones"]])
+    np.testing.assert_allclose(got, sub["forces"], atol=1e-12 * np.abs(sub["forces"]).max())
+    nodes, tau = sv.wall_shear("reaction")
+    np.testing.assert_array_equal(nodes, sub["reaction_nodes"])
+    np.testing.assert_allclose(tau, sub["reaction_tau"],
+                               atol=1e-11 * np.abs(sub["reaction_tau"]).max())
