@@ -216,3 +216,21 @@ def test_segmented_fgmres_converges_every_segment_on_its_own():
         ref = xe[o:o + n]
         np.testing.assert_allclose(x.numpy()[o:o + n], ref, atol=1e-6 * np.abs(ref).max())
         o += n
+
+
+def test_flow_rate_table_is_periodic_and_exact():
+    """A flow-rate inlet given as a periodic ``[(t, Q), ...]`` table (the reference's
+    ``_Signal``, ``zvcfd/lumped.py:57-70``): linear between entries, repeating with the period
+    of its last time, and the discrete inflow equal to ``rho Q(t)``."""
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.mesh import pipe
+
+    m = pipe(1e-3, 3e-3, n_core=4, n_ring=2, n_axial=3, kind="tet")
+    z = {zz.name: k for k, zz in m.zones.items()}
+    table = [(0.0, 1e-6), (0.3, 4e-6), (0.8, 1e-6)]
+    bcs = {z["inlet"]: {"kind": "velocity", "flow_rate": table},
+           z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    b = Boundary(m, bcs, 1060.0)
+    for t, q in ((0.0, 1e-6), (0.15, 2.5e-6), (0.3, 4e-6), (0.55, 2.5e-6), (0.95, 2.5e-6)):
+        b.update(t)
+        assert abs(-b.inflow.sum() - 1060.0 * q) < 1e-12 * 1060.0 * q
