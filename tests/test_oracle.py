@@ -182,3 +182,44 @@ def test_oracle_acm_fgmres_solves_an_assembled_system():
     X, R = x.reshape(-1, 4), spl.spsolve(A.tocsc(), b.reshape(-1)).reshape(-1, 4)
     assert np.abs(X[:, :3] - R[:, :3]).max() < 1e-5 * np.abs(R[:, :3]).max()
     assert np.abs(X[:, 3] - R[:, 3]).max() < 1e-5 * np.ptp(R[:, 3])
+
+
+@pytest.mark.parametrize("name", ["pipe_tet_si", "curved_cy"])
+def test_oracle_boundary_pass_keeps_the_solution(name):
+    """The restated boundary pass: symmetric elimination and the dimensionless row scaling
+    leave the solution of the Dirichlet system unchanged, the eliminated columns are empty,
+    fixed rows are scaled unit rows, and the residual sums are those of the state."""
+    import scipy.sparse.linalg as spl
+
+    from fixtures import fluid_of, mesh_of, pipe_bcs
+    from oracle.fv import OracleSolver
+
+    g = load(name)
+    m = mesh_of(g)
+    s = OracleSolver(m, fluid_of(g), pipe_bcs(name, g, m), advection=1.0)
+    s.solve(max_iterations=3, tol=0.0)
+    dirichlet, b_dir = s.assemble()
+    raw, b_raw = s.raw
+    X = np.concatenate([s.U, s.P[:, None]], 1)
+    ref = spl.spsolve(s.to_csr(dirichlet).tocsc(), b_dir.reshape(-1))
+    for eliminate in (True, False):
+        data, b, scale, stats = s.boundary_pass(raw, b_raw, X, eliminate=eliminate)
+        x = spl.spsolve(s.to_csr(data).tocsc(), b.reshape(-1))
+        np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max())
+        fixed = np.concatenate([s.vel_fixed_comp, s.p_fixed[:, None]], 1)
+        rows = np.repeat(np.arange(s.N), np.diff(s.indptr))
+        if eliminate:                      # free rows keep nothing in known columns
+            for r in range(4):
+                for c in range(4):
+                    assert np.all(data[fixed[s.indices, c] & ~fixed[rows, r], r, c] == 0.0)
+        dpos = s.diagonal_positions()
+        for r in range(4):
+            on = np.flatnonzero(fixed[:, r])
+            np.testing.assert_allclose(data[dpos[on], r, r], scale[on, r], rtol=1e-15)
+    # residual sums of the free rows, computed directly from the Dirichlet system
+    res = (b_dir.reshape(-1) - s.to_csr(dirichlet) @ X.reshape(-1)).reshape(-1, 4)
+    norm = np.concatenate([np.repeat(s.aP[:, None], 3, 1),
+                           (s.fluid.rho * s.V ** (2 / 3))[:, None]], 1)
+    v = np.where(fixed, 0.0, np.abs(res) / norm)
+    np.testing.assert_allclose(stats["max"], v.max(0), rtol=1e-10, atol=1e-300)
+    np.testing.assert_allclose(stats["sq"], (v * v).sum(0), rtol=1e-10, atol=1e-300)
