@@ -41,7 +41,8 @@ def node_graph(mesh):
 
 def element_keys(E: int) -> np.ndarray:
     """A hash of the element index in the high 32 bits, the index in the low 32
-    (``zvcfd/fv/fast.py:84-92``): distinct keys in a pseudo-random order."""
+    (``zvcfd/fv/fast.py:84-92``): distinct keys in a pseudo-random order. The hash is the
+    SplitMix64 output function (Steele, Lea and Flood 2014) with its published constants."""
     e = np.arange(E, dtype=np.uint64)
     with np.errstate(over="ignore"):
         z = e + np.uint64(0x9E3779B97F4A7C15)

@@ -65,7 +65,9 @@ int bits_for(unsigned long long v) {
 // ------------------------------------------------------------------------ colouring
 
 // A hash of the element index in the high 32 bits, the index in the low 32
-// (zvcfd/fv/fast.py:84-92): distinct keys in a pseudo-random order.
+// (zvcfd/fv/fast.py:84-92): distinct keys in a pseudo-random order. The hash is the
+// SplitMix64 output function (Steele, Lea and Flood, OOPSLA 2014; these are its published
+// constants), which the colouring must share with the reference to come out the same.
 __global__ void k_colour_keys(long long E, unsigned long long *__restrict__ key) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
