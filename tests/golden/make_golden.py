@@ -15,7 +15,8 @@ coefficients and Carreau-Yasuda viscosity (``lumped``); the backflow box with
 and without stabilisation (``backflow``); zone forces, flows and both wall-shear
 methods of two converged cases (``forces``); WSS time statistics (``wss``);
 the manufactured Carreau-Yasuda outlet (``gn_outlet``); developed inlet
-profiles and a pipe with the default flow-rate inlet (``profiles``). A single file is
+profiles and a pipe with the default flow-rate inlet (``profiles``); uneven BDF2 steps of
+an oscillating pipe (``variable_steps``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -437,6 +438,25 @@ def profiles_case() -> dict:
     return out
 
 
+def variable_steps_case() -> dict:
+    """The reference's variable-step BDF2 case (``tests/test_fv_boundaries.py:281-300``): a
+    hexahedral tube driven by an oscillating inlet pressure (Womersley number about 4), six
+    steps of uneven size, solved by the reference's CPU solver with lagged Rhie-Chow."""
+    R = 0.5
+    w = 2 * np.pi
+    nu = R * R * w / 16
+    m = tube(R, 0.5, n_core=2, n_ring=2, n_axial=2, kind="hex")
+    z = {b.name: k for k, b in m.zones.items()}
+    bcs = {z["inlet"]: {"kind": "pressure",
+                        "value": lambda x, t: 0.5 * np.cos(w * t) * np.ones(len(x))},
+           z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    steps = np.array([0.05, 0.08, 0.04, 0.06, 0.03, 0.07])
+    s = ReferenceSolver(m, Fluid(1.0, nu), bcs, advection=1.0, lag_rhie_chow=True)
+    rep = s.solve_transient(list(steps), loops=60, tol=1e-12)
+    return dict(mesh_arrays(m), U=s.U.copy(), P=s.P.copy(), steps=steps, nu=nu, omega=w,
+                converged=rep.converged)
+
+
 def lumped_case() -> dict:
     """The reference's RCR model (``zvcfd/lumped.py:181-218``): steady coefficients, and the
     step coefficients and committed pressures of 40 steps under a pulsatile outflow, for the
@@ -483,6 +503,10 @@ def main():
                 tag = f"kernel_{name}_{'gn' if gn else 'newt'}_{'dt' if dt else 'steady'}"
                 np.savez_compressed(HERE / f"{tag}.npz", **kernel_case(name, gn, dt))
         print("wrote kernels")
+        return
+    if sys.argv[1:] == ["variable_steps"]:
+        np.savez_compressed(HERE / "variable_steps.npz", **variable_steps_case())
+        print("wrote variable_steps")
         return
     if sys.argv[1:] == ["profiles"]:
         np.savez_compressed(HERE / "profiles.npz", **profiles_case())
@@ -546,6 +570,8 @@ def main():
     print("wrote gn_outlet")
     np.savez_compressed(HERE / "profiles.npz", **profiles_case())
     print("wrote profiles")
+    np.savez_compressed(HERE / "variable_steps.npz", **variable_steps_case())
+    print("wrote variable_steps")
 
 
 if __name__ == "__main__":

@@ -223,3 +223,24 @@ def test_oracle_boundary_pass_keeps_the_solution(name):
     v = np.where(fixed, 0.0, np.abs(res) / norm)
     np.testing.assert_allclose(stats["max"], v.max(0), rtol=1e-10, atol=1e-300)
     np.testing.assert_allclose(stats["sq"], (v * v).sum(0), rtol=1e-10, atol=1e-300)
+
+
+def test_oracle_variable_steps_match_reference():
+    """Six uneven BDF2 steps of the reference's oscillating-pressure tube
+    (``tests/test_fv_boundaries.py:281-300``): the oracle's variable-step coefficients and time
+    levels reach the reference's fields."""
+    from fixtures import mesh_of
+    from oracle.fv import OracleSolver
+    from zvcfd_b200.fluid import Fluid
+
+    g = load("variable_steps")
+    m = mesh_of(g)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    w = float(g["omega"])
+    bcs = {z["inlet"]: {"kind": "pressure",
+                        "value": lambda x, t: 0.5 * np.cos(w * t) * np.ones(len(x))},
+           z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    s = OracleSolver(m, Fluid(1.0, float(g["nu"])), bcs, advection=1.0)
+    s.solve_transient(list(g["steps"]), loops=60, tol=1e-12)
+    np.testing.assert_allclose(s.U, g["U"], atol=1e-11)
+    np.testing.assert_allclose(s.P, g["P"], atol=1e-11 * max(np.ptp(g["P"]), 1e-30))
