@@ -244,3 +244,37 @@ def test_oracle_variable_steps_match_reference():
     s.solve_transient(list(g["steps"]), loops=60, tol=1e-12)
     np.testing.assert_allclose(s.U, g["U"], atol=1e-11)
     np.testing.assert_allclose(s.P, g["P"], atol=1e-11 * max(np.ptp(g["P"]), 1e-30))
+
+
+@pytest.mark.parametrize("stokes", [True, False])
+def test_oracle_symmetry_plane_reproduces_the_full_channel(stokes):
+    """The reference's half-channel property (``tests/test_fv_reference.py:105-135``): a
+    channel of height 1 with a symmetry plane on top equals the lower half of the channel of
+    height 2 with two walls, to round-off, with symmetry planes on both z faces too."""
+    from oracle.fv import OracleSolver
+    from zvcfd_b200.fluid import Fluid
+    from zvcfd_b200.mesh import box
+
+    halves = {}
+    for H, ny in ((2.0, 8), (1.0, 4)):
+        m = box((6, ny, 2), (3.0, H, 0.5), kind="hex")
+        z = {zz.name: k for k, zz in m.zones.items()}
+
+        def inflow(x):
+            u = np.zeros((len(x), 3))
+            u[:, 0] = x[:, 1] * (2.0 - x[:, 1])
+            return u
+
+        bcs = {z["xmin"]: {"kind": "velocity", "value": inflow},
+               z["xmax"]: {"kind": "pressure", "value": 0.0}, z["ymin"]: {"kind": "wall"},
+               z["zmin"]: {"kind": "symmetry"}, z["zmax"]: {"kind": "symmetry"},
+               z["ymax"]: {"kind": "wall"} if H == 2.0 else {"kind": "symmetry"}}
+        s = OracleSolver(m, Fluid(1.0, 0.5), bcs, stokes=stokes)
+        assert s.solve(max_iterations=60, tol=1e-12)["converged"]
+        q = s.zone_flows()
+        assert abs(sum(q.values())) < 1e-13 * abs(q[z["xmin"]])
+        lower = m.nodes[:, 1] <= 1.0 + 1e-9
+        order = np.lexsort(np.round(m.nodes[lower] * 1e6).astype(np.int64).T[::-1])
+        halves[H] = (s.U[lower][order], s.P[lower][order])
+    np.testing.assert_allclose(halves[1.0][0], halves[2.0][0], atol=1e-12)
+    np.testing.assert_allclose(halves[1.0][1], halves[2.0][1], atol=1e-12)
