@@ -278,3 +278,50 @@ def test_oracle_symmetry_plane_reproduces_the_full_channel(stokes):
         halves[H] = (s.U[lower][order], s.P[lower][order])
     np.testing.assert_allclose(halves[1.0][0], halves[2.0][0], atol=1e-12)
     np.testing.assert_allclose(halves[1.0][1], halves[2.0][1], atol=1e-12)
+
+
+@pytest.mark.parametrize("kind,perturb", [("tet", 0.25), ("tet", 0.0), ("wedge", 0.0),
+                                          ("hex", 0.0)])
+def test_oracle_hydrostatic_is_exact(kind, perturb):
+    """The reference's exactness check (``tests/test_fv_reference.py:25-36``): at rest, a
+    uniform body force balanced by a linear pressure, to round-off. The lagged Rhie-Chow
+    iteration reaches it as its fixed point (the reference's implicit form in one solve)."""
+    from oracle.fv import OracleSolver
+    from zvcfd_b200.fluid import Fluid
+    from zvcfd_b200.mesh import box
+
+    m = box((5, 5, 5), kind=kind, perturb=perturb, seed=1)
+    g = np.array([0.3, -1.1, 0.7])
+    p = m.nodes @ g
+    s = OracleSolver(m, Fluid(), {z: {"kind": "wall"} for z in m.zones}, stokes=True,
+                     source=lambda x: np.broadcast_to(g, (len(x), 3)),
+                     reference_pressure=(0, float(p[0])))
+    s.solve(max_iterations=200, tol=0.0)
+    assert np.abs(s.U).max() < 1e-12
+    assert np.abs(s.P - p).max() < 1e-11
+
+
+@pytest.mark.parametrize("perturb", [0.0, 0.2])
+@pytest.mark.parametrize("kind", ["tet", "wedge", "hex"])
+def test_oracle_couette_is_exact_on_affine_elements(kind, perturb):
+    """A linear shear flow (``tests/test_fv_reference.py:39-60``): exact on every affine
+    element (all tetrahedra, undistorted wedges and hexahedra), close on distorted ones."""
+    from oracle.fv import OracleSolver
+    from zvcfd_b200.fluid import Fluid
+    from zvcfd_b200.mesh import box
+
+    def shear(x):
+        u = np.zeros((len(x), 3))
+        u[:, 0] = 0.5 + 2.0 * x[:, 2] - x[:, 1]
+        return u
+
+    m = box((4, 4, 4), kind=kind, perturb=perturb, seed=2)
+    s = OracleSolver(m, Fluid(1.0, 0.7), {z: {"kind": "velocity", "value": shear}
+                                          for z in m.zones}, stokes=True,
+                     reference_pressure=(0, 0.0))
+    s.solve(max_iterations=3)
+    err = np.abs(s.U - shear(m.nodes)).max() / 2.5
+    affine = kind == "tet" or perturb == 0
+    assert err < (1e-12 if affine else 5e-4)
+    if affine:
+        assert np.abs(s.P).max() < 1e-10
