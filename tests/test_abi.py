@@ -42,3 +42,39 @@ def test_tables_header_is_current():
     from zvcfd_b200.topology import HEADER_PATH, header_source
 
     assert HEADER_PATH.read_text() == header_source()
+
+
+def _prototypes():
+    """``{name: [parameter type strings]}`` of every prototype in ``include/*.h``."""
+    out = {}
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"\b(zvfv_\w+)\s*\(([^;{]*?)\)\s*;", text):
+            params = [p.strip() for p in m.group(2).split(",")]
+            out[m.group(1)] = [] if params in ([""], ["void"]) else params
+    return out
+
+
+def test_ctypes_signatures_match_the_header():
+    """Each entry point's ctypes argument list has the header's parameter count, and each
+    parameter's kind agrees: a pointer for ``*`` parameters, a double for ``double``, a 64-bit
+    integer for ``int64_t``, a 32-bit one for ``int``."""
+    import ctypes as C
+
+    from zvcfd_b200._lib import _SIGNATURES
+
+    protos = _prototypes()
+    assert set(protos) == set(_SIGNATURES)
+    for name, params in protos.items():
+        args = _SIGNATURES[name][0]
+        assert len(args) == len(params), (name, len(args), len(params))
+        for a, p in zip(args, params):
+            if "*" in p:
+                assert a in (C.c_void_p, C.c_char_p) or a.__name__.startswith("LP_"), (name, p)
+            elif p.startswith("double"):
+                assert a is C.c_double, (name, p)
+            elif p.startswith("int64_t"):
+                assert a is C.c_int64, (name, p)
+            elif p.startswith("int"):
+                assert a is C.c_int, (name, p)
