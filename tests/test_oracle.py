@@ -325,3 +325,19 @@ def test_oracle_couette_is_exact_on_affine_elements(kind, perturb):
     assert err < (1e-12 if affine else 5e-4)
     if affine:
         assert np.abs(s.P).max() < 1e-10
+
+
+def test_oracle_steady_state_does_not_depend_on_the_false_time_step():
+    """The reference's check (``tests/test_fv_reference.py:165-179``): relaxing with a false
+    time step reaches the same steady state (the transient Rhie-Chow part cancels there)."""
+    from fixtures import fluid_of, mesh_of, pipe_bcs
+    from oracle.fv import OracleSolver
+
+    g = load("pipe_reference_tube")
+    m = mesh_of(g)
+    bcs = pipe_bcs("pipe_reference_tube", g, m)
+    for dt in (0.05, 0.5):
+        s = OracleSolver(m, fluid_of(g), bcs, advection=1.0, dt=dt)
+        assert s.solve(max_iterations=600, tol=1e-13)["converged"]
+        np.testing.assert_allclose(s.P, g["P"], atol=1e-10 * np.ptp(g["P"]))
+        np.testing.assert_allclose(s.U, g["U"], atol=1e-10 * np.abs(g["U"]).max())
