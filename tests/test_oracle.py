@@ -341,3 +341,40 @@ def test_oracle_steady_state_does_not_depend_on_the_false_time_step():
         assert s.solve(max_iterations=600, tol=1e-13)["converged"]
         np.testing.assert_allclose(s.P, g["P"], atol=1e-10 * np.ptp(g["P"]))
         np.testing.assert_allclose(s.U, g["U"], atol=1e-10 * np.abs(g["U"]).max())
+
+
+def test_oracle_lumped_outlet_reaches_its_0d_law():
+    """The oracle's lumped RCR outlet (implicit rows ``p_j - r Q = a``): at the steady state
+    the outlet pressure is ``a + r Q`` of the model's resting pair, and over BDF2 steps of a
+    pulsing inflow it follows the standalone 0-D model fed with the same flows (the laws of
+    the reference's ``tests/test_fv_boundaries.py:88-130``)."""
+    from fixtures import axial_parabola, fluid_of, mesh_of, pipe_bcs
+    from oracle.fv import OracleSolver
+    from zvcfd_b200.lumped import RCR
+
+    g = load("pipe_reference_tube")
+    m = mesh_of(g)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    bcs = pipe_bcs("pipe_reference_tube", g, m)
+    pulse = axial_parabola(float(g["radius"]), float(g["umax"]),
+                           pulse=lambda t: 1.0 + 0.5 * np.sin(2 * np.pi * t / 0.8))
+    bcs[z["inlet"]] = {"kind": "velocity", "value": pulse}
+    model = RCR(rp=0.5, c=1e-3, rd=2.0, pv=1.0)
+    bcs[z["outlet"]] = {"kind": "pressure", "lumped": model}
+    s = OracleSolver(m, fluid_of(g), bcs, advection=1.0)
+    assert s.solve(max_iterations=400, tol=1e-12)["converged"]
+    nodes = s._zone_nodes[z["outlet"]]
+    rho = s.fluid.rho
+    q = s.zone_flows()
+    a, r = RCR(rp=0.5, c=1e-3, rd=2.0, pv=1.0).steady_coefficients()
+    np.testing.assert_allclose(s.P[nodes], a + r * q[z["outlet"]] / rho, rtol=1e-12)
+    assert abs(sum(q.values())) < 1e-12 * sum(abs(v) for v in q.values())
+    alone = RCR(rp=0.5, c=1e-3, rd=2.0, pv=1.0)
+    alone.initialise(q[z["outlet"]] / rho, 0.0)
+    seen = []
+    for _ in range(3):
+        s.solve_transient(0.05, 1, loops=200, tol=1e-12)
+        Q = s.zone_flows()[z["outlet"]] / rho
+        np.testing.assert_allclose(s.P[nodes], alone.advance(Q, s.t, 0.05), rtol=1e-10)
+        seen.append(Q)
+    assert np.ptp(seen) > 0.05 * abs(seen[0])          # the flow did change
