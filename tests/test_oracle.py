@@ -378,3 +378,31 @@ def test_oracle_lumped_outlet_reaches_its_0d_law():
         np.testing.assert_allclose(s.P[nodes], alone.advance(Q, s.t, 0.05), rtol=1e-10)
         seen.append(Q)
     assert np.ptp(seen) > 0.05 * abs(seen[0])          # the flow did change
+
+
+def test_oracle_poiseuille_pipe_balances_mass_and_converges_at_second_order():
+    """The reference's ``tests/test_fv_reference.py:82-104`` on the oracle: a Stokes
+    Poiseuille pipe on hexahedra carries its inflow out to round-off, and its pressure gradient
+    approaches ``8 mu U / R^2`` at second order under refinement."""
+    from fixtures import axial_parabola
+    from oracle.fv import OracleSolver
+    from zvcfd_b200.fluid import Fluid
+    from zvcfd_b200.mesh import pipe
+
+    R, L = 0.5, 3.0
+    errors = []
+    for nc in (2, 4):
+        m = pipe(R, L, n_core=nc, n_ring=nc, n_axial=6 * nc, kind="hex")
+        z = {zz.name: k for k, zz in m.zones.items()}
+        s = OracleSolver(m, Fluid(), {z["inlet"]: {"kind": "velocity",
+                                                   "value": axial_parabola(R, 2.0)},
+                                      z["outlet"]: {"kind": "pressure", "value": 0.0},
+                                      z["wall"]: {"kind": "wall"}}, stokes=True)
+        assert s.solve(max_iterations=300, tol=1e-10)["converged"]
+        q = s.zone_flows()
+        assert abs(q[z["outlet"]] + q[z["inlet"]]) < 1e-12 * abs(q[z["inlet"]])
+        zc = m.nodes[:, 2]
+        drop = s.P[np.isclose(zc, 0.25 * L)].mean() - s.P[np.isclose(zc, 0.75 * L)].mean()
+        errors.append(abs(drop / (0.5 * L) / (8 / R ** 2) - 1))
+    assert errors[1] < 0.04
+    assert np.log2(errors[0] / errors[1]) > 1.8
