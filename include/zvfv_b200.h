@@ -179,7 +179,8 @@ int zvfv_fold(int64_t nrows, int width, const double *partial, const int32_t *op
  * library that every GPU loading it holds until exit, which limits n to 1..16,777,216 nodes;
  * larger n returns ZVFV_BAD_ARGUMENT with a message. The first call on each device looks up
  * that array's device address (with the device current) and should come before any stream
- * capture. Calls share the array: two calls that overlap on the GPU (different streams, no
+ * capture; the address is kept with the device's current context and looked up again when
+ * that context changes (after a device reset). Calls share the array: two calls that overlap on the GPU (different streams, no
  * ordering between them) race and give wrong statistics. Results equal zvfv_update followed by
  * zvfv_fold with ops {1, 1, 1, 2, 1} bit for bit. */
 int zvfv_update_noalloc(int64_t n, const double *x, double *U, double *P, double *stats,

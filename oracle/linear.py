@@ -81,6 +81,52 @@ def pairwise(n, indptr, indices, strength):
     return np.array(agg, np.int64), count
 
 
+def pairwise_arrays(n, indptr, indices, strength):
+    """:func:`pairwise` over whole arrays: the form the reference's own host aggregation takes
+    (``zvcfd/fv/linear.py:355-396``), used where the node-by-node form is too slow (the CPU
+    baseline at full size). Same rounds, picks, ties (the first maximum in column order) and
+    numbering, so the aggregates are equal to :func:`pairwise`'s (checked in the tests)."""
+    rows = np.repeat(np.arange(n), np.diff(np.asarray(indptr, np.int64)))
+    cols = np.asarray(indices, np.int64)
+    off = rows != cols
+    r, c, s = rows[off], cols[off], np.asarray(strength)[off]
+    agg = np.full(n, -1, np.int64)
+    count = 0
+
+    def first_pick(rr, cc, ss):
+        """Each row's strongest column (ties: the smallest column), -1 for rows without one."""
+        pick = np.full(n, -1, np.int64)
+        if len(rr):
+            order = np.lexsort((cc, -ss, rr))
+            head = np.ones(len(order), bool)
+            head[1:] = rr[order][1:] != rr[order][:-1]
+            pick[rr[order][head]] = cc[order][head]
+        return pick
+
+    for _ in range(4):
+        live = (agg[r] < 0) & (agg[c] < 0)
+        if not live.any():
+            break
+        best = first_pick(r[live], c[live], s[live])
+        i = np.flatnonzero(best >= 0)
+        j = best[i]
+        pair = (best[j] == i) & (i < j)
+        a, b = i[pair], j[pair]                       # ascending in a: numbered in its order
+        agg[a] = agg[b] = count + np.arange(len(a))
+        count += len(a)
+    free = np.flatnonzero(agg < 0)
+    if len(free):
+        reach = (agg[r] < 0) & (agg[c] >= 0)
+        join = first_pick(r[reach], c[reach], s[reach])[free]
+        joined = join >= 0
+        target = agg[join[joined]]
+        agg[free[joined]] = target
+        alone = free[~joined]
+        agg[alone] = count + np.arange(len(alone))
+        count += len(alone)
+    return agg, count
+
+
 def transpose_positions(indptr, indices):
     """Position of the entry (j, i) for every entry (i, j) of a structurally symmetric pattern."""
     n = len(indptr) - 1
@@ -92,7 +138,7 @@ def transpose_positions(indptr, indices):
     return pos
 
 
-def aggregate(indptr, indices, data, passes=2, mode=0):
+def aggregate(indptr, indices, data, passes=2, mode=0, matcher=None):
     """``passes`` pairwise passes with the graph coarsened between them by summing strengths
     per aggregate pair (``zvcfd/fv/linear.py:415-433``). Returns ``(agg, count)``. ``mode`` 2
     (not in the reference) averages each block norm with that of its transpose position."""
@@ -110,7 +156,7 @@ def aggregate(indptr, indices, data, passes=2, mode=0):
         dmask = rows == cols
         diag[rows[dmask]] = w[dmask]
         s = w / np.sqrt(np.maximum(diag[rows] * diag[cols], 1e-300))
-        a, count_new = pairwise(count, ptr, cols, s)
+        a, count_new = (matcher or pairwise)(count, ptr, cols, s)
         total = a[total]
         if p + 1 == passes:
             count = count_new
@@ -147,13 +193,22 @@ class ACM:
     aggregation, Galerkin block sums, damped block-Jacobi smoothing, a dense coarsest solve."""
 
     def __init__(self, *, smooth=2, omega=0.7, coarse=24, passes=2, mode=0, max_levels=25,
-                 coarse_sweeps=8):
+                 coarse_sweeps=8, matcher=None, rebuild_every=1):
         self.smooth, self.omega, self.coarse, self.passes = smooth, omega, coarse, passes
         self.mode, self.max_levels, self.coarse_sweeps = mode, max_levels, coarse_sweeps
+        self.matcher = matcher
+        # aggregates are kept between re-aggregations, the coefficients re-summed every set-up
+        # (the reference ACM's rebuild_every, zvcfd/fv/linear.py:456-470)
+        self.rebuild_every, self._setups, self._aggs = rebuild_every, 0, None
 
     def setup(self, indptr, indices, data):
         self.levels = []
+        rebuild = self._aggs is None or self._setups % self.rebuild_every == 0
+        self._setups += 1
+        if rebuild:
+            self._aggs = []
         ptr, idx, dat = np.asarray(indptr), np.asarray(indices, np.int64), np.asarray(data)
+        depth = 0
         while True:
             n = len(ptr) - 1
             A = bsr(ptr, idx, dat, n).tocsr()
@@ -170,9 +225,16 @@ class ACM:
                 break
             if len(self.levels) >= self.max_levels:
                 break
-            agg, nc = aggregate(ptr, idx, dat, self.passes, self.mode)
-            if nc >= 0.9 * n or nc < 1:
+            if rebuild:
+                agg, nc = aggregate(ptr, idx, dat, self.passes, self.mode, self.matcher)
+                if nc >= 0.9 * n or nc < 1:
+                    break
+                self._aggs.append((agg, nc))
+            elif depth < len(self._aggs):
+                agg, nc = self._aggs[depth]
+            else:
                 break
+            depth += 1
             L["agg"], L["nc"] = agg, nc
             ptr, idx, dat = galerkin(ptr, idx, dat, agg, nc)
         return self

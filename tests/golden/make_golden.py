@@ -1,8 +1,9 @@
 """Generate the golden vectors of the coupled FV path by running the reference itself.
 
-Run once, in a container where the reference is importable:
+Run once, in a container where the reference is importable, with ``ZVCFD_REFERENCE`` naming
+the reference's source tree:
 
-    PYTHONPATH=/root/reference:. PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
+    PYTHONPATH=$ZVCFD_REFERENCE:. PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
 
 It writes ``tests/golden/*.npz``: element tables, and for six distorted test
 meshes (every element type) the reference's node volumes, nodal gradients,
@@ -16,7 +17,8 @@ and without stabilisation (``backflow``); zone forces, flows and both wall-shear
 methods of two converged cases (``forces``); WSS time statistics (``wss``);
 the manufactured Carreau-Yasuda outlet (``gn_outlet``); developed inlet
 profiles and a pipe with the default flow-rate inlet (``profiles``); uneven BDF2 steps of
-an oscillating pipe (``variable_steps``). A single file is
+an oscillating pipe (``variable_steps``); a mid-size curved Carreau-Yasuda tube
+(``curved_mid``, about 6k nodes, the bench tube's cross-section coarsened). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -29,7 +31,12 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = "/root/reference"          # the reference's source tree (also on PYTHONPATH)
+import os  # noqa: E402
+
+# the reference's source tree (also on PYTHONPATH); its validation helpers live beneath it
+REFERENCE = os.environ.get("ZVCFD_REFERENCE", "")
+if not REFERENCE:
+    raise SystemExit("set ZVCFD_REFERENCE to the reference's source tree")
 sys.path.insert(0, str(HERE.parents[1]))
 
 from zvcfd.fv.geometry import topology  # noqa: E402  (the reference)
@@ -201,6 +208,34 @@ def pipe_cases() -> dict:
                               iterations=rep.iterations, flow_rate=1e-6,
                               cy=np.array([cy.mu_0, cy.mu_inf, cy.lam, cy.a, cy.n]))
     return cases
+
+
+def curved_mid_case() -> dict:
+    """Converged fields of a mid-size curved Carreau-Yasuda tube (the headline tube's geometry
+    and fluid at about 6k nodes: hexahedral core, three wedge wall layers, 1 ml/s), solved by
+    the reference's CPU solver with lagged Rhie-Chow (SuperLU per linearisation,
+    ``zvcfd/fv/reference.py:952-980``). The advection blend is fixed (1.0), as in the other
+    converged goldens: a limiter frozen at iteration 10 would tie the converged state to the
+    linear solver's path to that iteration, which an inexact Krylov solve does not share."""
+    cm = zmesh.curved_tube(2e-3, 20e-3, np.pi / 2, n_core=8, n_ring=5, n_axial=24, layers=3,
+                           growth=0.8)
+    um = to_reference(cm)
+    z = {zz.name: k for k, zz in cm.zones.items()}
+
+    def shape(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / (2e-3) ** 2
+        return np.clip(1 - r2, 0, None)
+
+    bcs = {z["inlet"]: {"kind": "velocity", "flow_rate": 1e-6, "profile": shape},
+           z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    cy = CarreauYasuda()
+    s = ReferenceSolver(um, Fluid(1060.0, 0.00345, viscosity=cy), bcs, advection=1.0,
+                        lag_rhie_chow=True)
+    rep = s.solve(max_iterations=300, tol=1e-11)
+    assert rep.converged, rep.iterations
+    return dict(mesh_arrays(cm), U=s.U, P=s.P, rho=1060.0, mu=0.00345,
+                iterations=rep.iterations, flow_rate=1e-6,
+                cy=np.array([cy.mu_0, cy.mu_inf, cy.lam, cy.a, cy.n]))
 
 
 def transient_case() -> dict:
@@ -503,6 +538,10 @@ def main():
                 tag = f"kernel_{name}_{'gn' if gn else 'newt'}_{'dt' if dt else 'steady'}"
                 np.savez_compressed(HERE / f"{tag}.npz", **kernel_case(name, gn, dt))
         print("wrote kernels")
+        return
+    if sys.argv[1:] == ["curved_mid"]:
+        np.savez_compressed(HERE / "curved_mid.npz", **curved_mid_case())
+        print("wrote curved_mid")
         return
     if sys.argv[1:] == ["variable_steps"]:
         np.savez_compressed(HERE / "variable_steps.npz", **variable_steps_case())

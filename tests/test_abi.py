@@ -31,8 +31,8 @@ def test_library_reports_errors_without_a_gpu():
     from zvcfd_b200 import _lib
 
     assert _lib.lib.zvfv_version() >= 1
-    assert _lib.lib.zvfv_record_doubles(3) == 728          # hex: 2*24*3 + 24*8*3 + 8
-    assert _lib.lib.zvfv_record_doubles(0) == 88            # tet (one gradient set)
+    assert _lib.lib.zvfv_record_doubles(3) == 368          # hex: 2*24*3 + 24*9 + 8
+    assert _lib.lib.zvfv_record_doubles(0) == 85            # tet: 2*12*3 + 9 + 4 (one Jacobian)
     # argument checks run before any CUDA call
     rc = _lib.lib.zvfv_gradient(10, 5, 0, None, None, None, None, None, None, None)
     assert rc == 1 and b"nc" in _lib.lib.zvfv_last_error()

@@ -18,6 +18,26 @@ def test_tables_match_reference():
         np.testing.assert_array_equal(t.weights, g[f"{k}_W"])
 
 
+def test_kernel_tables_restate_the_reference_tables():
+    """The element kernels' forms of the tables (corner node masks, flux point as the fastest
+    index) hold the same numbers: each triangle corner is the plain mean of its mask's nodes,
+    and the transposed shape functions and derivatives are the reference's."""
+    from zvcfd_b200.topology import _kernel_tables
+
+    g = load("tables")
+    for k in KINDS:
+        t = tables(k)
+        arrays = {name: a for name, a, _ in _kernel_tables(t)}
+        W = g[f"{k}_W"][g[f"{k}_tris"]]                          # (n_ip, 3, n)
+        bits = (arrays["MASK"][..., None] >> np.arange(t.n)) & 1
+        np.testing.assert_array_equal(W > 0, bits.astype(bool))
+        np.testing.assert_allclose(W, bits / bits.sum(-1, keepdims=True), rtol=0, atol=1e-16)
+        np.testing.assert_array_equal(arrays["NT"], g[f"{k}_N"].T)
+        dnt = arrays["DNT"].reshape(t.n, 3, t.n_ip)
+        np.testing.assert_array_equal(dnt.transpose(2, 0, 1), g[f"{k}_dN"])
+        np.testing.assert_array_equal(arrays["EDGE"], g[f"{k}_edges"])
+
+
 @pytest.mark.parametrize("variant", KERNEL_VARIANTS)
 @pytest.mark.parametrize("name", KERNEL_MESHES)
 def test_oracle_matches_reference_kernels(name, variant):
@@ -155,6 +175,42 @@ def test_symmetrised_strength_keeps_pairwise_coarsening_under_convection():
     _, symmetric = aggregate(ip, cols, data, 2, 2)
     assert one_sided > 0.5 * n
     assert symmetric < 0.25 * n
+
+
+def test_array_matching_equals_the_node_by_node_matching():
+    """The whole-array pairwise matching (the CPU baseline's) picks, ties and numbers the
+    aggregates exactly as the node-by-node restatement: on an assembled golden system (both
+    strength modes, both passes) and on random strengths with many exact ties."""
+    from fixtures import fluid_of, mesh_of, pipe_bcs
+    from oracle.fv import OracleSolver
+    from oracle.linear import aggregate, pairwise, pairwise_arrays
+
+    g = load("pipe_tet_si")
+    m = mesh_of(g)
+    s = OracleSolver(m, fluid_of(g), pipe_bcs("pipe_tet_si", g, m), advection=1.0)
+    s.solve(max_iterations=2, tol=0.0)
+    data, _ = s.assemble()
+    for mode in (0, 2):
+        a1, n1 = aggregate(s.indptr, s.indices, data, 2, mode)
+        a2, n2 = aggregate(s.indptr, s.indices, data, 2, mode, pairwise_arrays)
+        assert n1 == n2
+        np.testing.assert_array_equal(a1, a2)
+    rng = np.random.default_rng(3)
+    n = 400
+    for trial in range(5):
+        dense = rng.random((n, n)) < 0.02
+        dense = dense | dense.T | np.eye(n, dtype=bool)
+        if trial == 4:
+            dense[:50] = dense[:, :50] = False           # isolated rows: singletons
+            dense[np.arange(n), np.arange(n)] = True
+        rows, cols = np.nonzero(dense)
+        ptr = np.zeros(n + 1, np.int64)
+        np.cumsum(np.bincount(rows, minlength=n), out=ptr[1:])
+        strength = rng.integers(0, 4, len(cols)).astype(float)     # many ties
+        a1, n1 = pairwise(n, ptr, cols, strength)
+        a2, n2 = pairwise_arrays(n, ptr, cols, strength)
+        assert n1 == n2
+        np.testing.assert_array_equal(a1, a2)
 
 
 def test_oracle_acm_fgmres_solves_an_assembled_system():

@@ -322,12 +322,43 @@ constexpr long long NOALLOC_MAX_NODES = NOALLOC_MAX_PARTIAL_ROWS * UPD_THREADS; 
 static __device__ __align__(256) double g_update_scratch[NOALLOC_MAX_PARTIAL_ROWS * 5];
 static __device__ __align__(256) int g_update_fold_ops[5] = {1, 1, 1, 2, 1};
 
-// Device addresses of the two arrays, looked up once per device with that device current.
-// In host code the arrays' names stand for host-side shadows, never for device memory.
+// Device addresses of the two arrays, looked up once per device with that device current and
+// kept with the CUDA context they belong to. In host code the arrays' names stand for
+// host-side shadows, never for device memory. A context that is torn down and recreated
+// (cudaDeviceReset, or a host program that destroys the primary context) reloads the module
+// at new addresses, so a cached entry is used only while the device's current context is the
+// one it was looked up in; otherwise the addresses are looked up again.
 struct NoallocScratch {
     double *partial = nullptr;
     int *ops = nullptr;
+    void *context = nullptr;
 };
+
+// The calling thread's current driver context (null before the runtime has made one), through
+// the runtime's driver entry point so that the library needs no link to the driver library.
+int current_context(void **ctx) {
+    using CtxGetCurrent = int (*)(void **);
+    static CtxGetCurrent get = nullptr;
+    static std::once_flag once;
+    static cudaError_t found = cudaSuccess;
+    std::call_once(once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        found = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+        if (found == cudaSuccess && q == cudaDriverEntryPointSuccess) get = (CtxGetCurrent)fn;
+    });
+    if (!get) {
+        set_error("update_noalloc: the driver entry point cuCtxGetCurrent is unavailable (%s)",
+                  cudaGetErrorString(found));
+        return CUDA_FAILURE;
+    }
+    *ctx = nullptr;
+    if (get(ctx) != 0) {
+        set_error("update_noalloc: cuCtxGetCurrent failed");
+        return CUDA_FAILURE;
+    }
+    return OK;
+}
 
 int noalloc_scratch(NoallocScratch *out) {
     constexpr int MAX_DEVICES = 64;
@@ -340,9 +371,11 @@ int noalloc_scratch(NoallocScratch *out) {
                   MAX_DEVICES);
         return BAD_ARGUMENT;
     }
+    void *ctx = nullptr;
+    if (int rc = current_context(&ctx)) return rc;
     std::lock_guard<std::mutex> guard(lock);
     NoallocScratch &e = table[dev];
-    if (!e.partial) {
+    if (!e.partial || !ctx || ctx != e.context) {
         void *partial = nullptr, *ops = nullptr;
         if (int rc = cuda_status(cudaGetSymbolAddress(&partial, g_update_scratch),
                                  "update_noalloc: cudaGetSymbolAddress(scratch)"))
@@ -350,8 +383,11 @@ int noalloc_scratch(NoallocScratch *out) {
         if (int rc = cuda_status(cudaGetSymbolAddress(&ops, g_update_fold_ops),
                                  "update_noalloc: cudaGetSymbolAddress(fold ops)"))
             return rc;
+        // the lookup made the runtime's context current if there was none yet
+        if (int rc = current_context(&ctx)) return rc;
         e.ops = static_cast<int *>(ops);
         e.partial = static_cast<double *>(partial);
+        e.context = ctx;
     }
     *out = e;
     return OK;

@@ -1,7 +1,7 @@
 // Wall shear stress at wall nodes from the wall integration points of their sub-faces
 // (zvcfd/fv/wall.py:66-137): per ip, grad u from the owning element's shape gradients, the
 // traction t = mu (grad u + grad u^T) . n, its tangential part, area-weighted per node.
-#include "element.cuh"
+#include "fvmath.cuh"
 
 namespace zvfv {
 namespace {

@@ -152,8 +152,17 @@ class ElementTables:
 
     @property
     def record_doubles(self) -> int:
-        """Doubles in a stored geometry record: areas, centroids, gradients, sub-volumes."""
-        return 2 * self.n_ip * 3 + self.n_grad * self.n * 3 + self.n
+        """Doubles in a stored geometry record: flux-point areas and centroids, the inverse
+        Jacobian of the element map at each flux point (one for tetrahedra), the
+        sub-control volumes."""
+        return 2 * self.n_ip * 3 + self.n_grad * 9 + self.n
+
+    @property
+    def corner_masks(self) -> np.ndarray:
+        """``(n_ip, 3)`` bit masks of the element nodes whose mean is each corner of a flux
+        point's triangle (edge midpoint, face centroid, element centroid)."""
+        w = self.weights[self.tris]                              # (n_ip, 3, n)
+        return ((w > 0) * (1 << np.arange(self.n))).sum(-1).astype(np.int64)
 
 
 @lru_cache(maxsize=None)
@@ -196,11 +205,6 @@ def tables(kind: str) -> ElementTables:
     return ElementTables(kind, n, 2 * ne, edge_ip, tris, W, xi, N, dN, ips, sgn)
 
 
-def epb(n: int) -> int:
-    """Elements per thread block of the per-element kernels: ``n^2`` threads each, ~128."""
-    return max(1, 128 // (n * n))
-
-
 # ---------------------------------------------------------------- header generation
 
 def _c_array(name: str, a: np.ndarray, ctype: str) -> str:
@@ -213,18 +217,27 @@ def _c_array(name: str, a: np.ndarray, ctype: str) -> str:
     return f"static __constant__ {ctype} {name}{dims} = {{{body}}};"
 
 
-_TABLES = (("EDGE", "edge", "int"), ("TRIS", "tris", "int"), ("WPT", "weights", "double"),
-           ("NIPF", "N_ip", "double"), ("DN", "dN_ip", "double"), ("IPS", "node_ips", "int"),
-           ("SGN", "node_sgn", "double"))
+def _kernel_tables(t: ElementTables):
+    """The tables as the element kernels index them: lanes of a warp take one flux point each,
+    so every per-flux-point table has the flux point as its fastest index."""
+    return (("EDGE", t.edge, "int"),                               # (n_ip, 2)
+            ("MASK", t.corner_masks, "int"),                       # (n_ip, 3)
+            ("NT", t.N_ip.T, "double"),                            # (n, n_ip)
+            ("DNT", t.dN_ip.transpose(1, 2, 0).reshape(t.n * 3, t.n_ip), "double"),
+            ("IPS", t.node_ips, "int"),                            # (n, MAXI)
+            ("SGN", t.node_sgn, "int"))                            # (n, MAXI) +1 / -1 / 0
 
 
 def header_source() -> str:
     """CUDA source of ``topology_tables.h``.
 
-    Per type: the tables as ``__constant__`` arrays (``k<KIND>_<TABLE>``), and a
-    ``Topo<K>`` traits struct with the sizes as compile-time constants and
-    pointers to its tables, so kernels templated on the type can size their
-    shared memory and unroll their loops.
+    Per type: the tables as ``__constant__`` arrays (``k<KIND>_<TABLE>``) and a ``Topo<K>``
+    traits struct with the sizes as compile-time constants and pointers to its tables, so
+    that kernels templated on the type size their staging and unroll their loops:
+    ``EDGE`` the edge nodes of each flux point, ``MASK`` the nodes averaged into each corner
+    of its triangle, ``NT[q][s]`` the shape function of node q at flux point s, ``DNT[q*3+d][s]``
+    its derivative along parametric axis d, ``IPS``/``SGN`` the flux points at each node and
+    the side the node is on (+1 the edge's first node, -1 its second).
     """
     out = ["// Generated by zvcfd_b200.topology.write_header(); do not edit.",
            "// Element tables of the median-dual discretisation (flux points, shape functions).",
@@ -235,23 +248,20 @@ def header_source() -> str:
     for kind in KINDS:
         t = tables(kind)
         K = kind.upper()
-        for cname, attr, ctype in _TABLES:
-            out.append(_c_array(f"k{K}_{cname}", getattr(t, attr), ctype))
+        for cname, arr, ctype in _kernel_tables(t):
+            out.append(_c_array(f"k{K}_{cname}", arr, ctype))
         out.append(f"template <> struct Topo<{K}> {{")
         out.append(f"    static constexpr int N = {t.n};")
         out.append(f"    static constexpr int NIP = {t.n_ip};")
-        out.append(f"    static constexpr int NPTS = {t.n_pts};")
         out.append(f"    static constexpr int CONSTG = {int(t.const_gradient)};")
         out.append(f"    static constexpr int NG = {t.n_grad};")
         out.append(f"    static constexpr int REC = {t.record_doubles};")
-        out.append(f"    static constexpr int EPB = {epb(t.n)};")
         out.append(f"    __device__ static const int (*edge())[2] {{ return k{K}_EDGE; }}")
-        out.append(f"    __device__ static const int (*tris())[3] {{ return k{K}_TRIS; }}")
-        out.append(f"    __device__ static const double (*wpt())[{t.n}] {{ return k{K}_WPT; }}")
-        out.append(f"    __device__ static const double (*nip())[{t.n}] {{ return k{K}_NIPF; }}")
-        out.append(f"    __device__ static const double (*dn())[{t.n}][3] {{ return k{K}_DN; }}")
+        out.append(f"    __device__ static const int (*mask())[3] {{ return k{K}_MASK; }}")
+        out.append(f"    __device__ static const double (*nt())[{t.n_ip}] {{ return k{K}_NT; }}")
+        out.append(f"    __device__ static const double (*dnt())[{t.n_ip}] {{ return k{K}_DNT; }}")
         out.append(f"    __device__ static const int (*ips())[MAXI] {{ return k{K}_IPS; }}")
-        out.append(f"    __device__ static const double (*sgn())[MAXI] {{ return k{K}_SGN; }}")
+        out.append(f"    __device__ static const int (*sgn())[MAXI] {{ return k{K}_SGN; }}")
         out.append("};")
         out.append("")
     out.append("}  // namespace zvfv")
@@ -270,5 +280,5 @@ def write_header(path: Path = HEADER_PATH) -> bool:
     return True
 
 
-__all__ = ["EDGES", "ElementTables", "FACES", "KINDS", "NODES_PER", "epb", "header_source",
+__all__ = ["EDGES", "ElementTables", "FACES", "KINDS", "NODES_PER", "header_source",
            "shape_functions", "tables", "write_header"]
