@@ -37,10 +37,11 @@ sys.path.insert(0, str(ROOT))
 METRIC = "FV outer-iteration time & block-SpMV GB/s, mixed vs FP64 at 1e-8 rel. residual"
 UNIT = "outer-iterations/s"
 WORKLOAD = "curved Carreau-Yasuda tube, 400,686 nodes (hex core + 5 wedge wall layers), steady"
-# DRAM bytes per algorithmic byte of the FP64 block SpMV (k_bsr_spmv<16>): ncu measured
-# 696,748,032 B read + 5,399,808 B written for 703,481,132 algorithmic bytes on the 211,551-node
-# tube; the traffic of the full matrix is this ratio times its algorithmic bytes
-SPMV_TRAFFIC_PER_ALGORITHMIC_BYTE = (696_748_032 + 5_399_808) / 703_481_132
+# DRAM bytes per algorithmic byte of one Gauss-Seidel pass on the finest level (the dominant
+# kernel), from an ncu capture of a smaller tube whose matrix is larger than L2; None until
+# captured. The traffic of the full pass is this ratio times its algorithmic bytes.
+GS_TRAFFIC_PER_ALGORITHMIC_BYTE = None
+GS_TRAFFIC_SOURCE = None
 
 
 def make_case(n_axial=285):
@@ -155,30 +156,60 @@ def spmv_roofline(solver, reps=20):
     return out, n, nnzb
 
 
-class CpuCase:
-    """The reference's CPU algorithm, restated by the oracle (NumPy assembly, a SuperLU solve
-    of each linearisation, mass flows: ``zvcfd/fv/reference.py:952-980``) on a shorter tube of
-    the same cross-section: the bounded CPU sample of the workload."""
+def host_info() -> dict:
+    """The host cores the CPU legs run on: count, model, thread settings."""
+    model = ""
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    blas = None
+    try:
+        from threadpoolctl import threadpool_info
 
-    def __init__(self, n_axial=3):
+        blas = sum(int(d.get("num_threads", 0)) for d in threadpool_info()
+                   if d.get("user_api") == "blas")
+    except Exception:
+        pass
+    return {"nproc": os.cpu_count(), "model": model, "blas_threads": blas,
+            "OMP_NUM_THREADS": os.environ.get("OMP_NUM_THREADS")}
+
+
+class CpuCase:
+    """The reference's CPU path for this workload, restated by the oracle: NumPy element assembly
+    of the lagged Rhie-Chow system (``zvcfd/fv/reference.py:654-806``) and each linearisation
+    solved by the reference's ACM inside FGMRES to ``linear_rtol`` 0.1 (``zvcfd/fv/linear.py:
+    328-518``, its defaults: 2 block-Jacobi sweeps, omega 0.7, coarsest 400 rows, two pairwise
+    passes, aggregates kept for 10 set-ups, restart 30), as SuperLU does not finish at this
+    size. NumPy's element-wise and SciPy's sparse kernels run on one thread."""
+
+    def __init__(self, n_axial=285):
         from oracle.fv import OracleSolver
+        from oracle.linear import ACM, pairwise_arrays
 
         m, fl, bcs = make_case(n_axial)
         self.n_nodes = m.n_nodes
         self.s = OracleSolver(m, fl, bcs)
+        self.acm = ACM(coarse=400, matcher=pairwise_arrays, rebuild_every=10)
+        self.linear_iterations = []
+
+    def _linear(self, data, b, x0):
+        from oracle.linear import fgmres
+
+        A = self.s.system_matrix(data).tocsr()
+        self.acm.setup(self.s.indptr, self.s.indices, data)
+        x, its, _, _ = fgmres(lambda v: A @ v, b, x0, self.acm.vcycle, rtol=0.1, restart=30,
+                              maxiter=200)
+        self.linear_iterations.append(int(its))
+        return x
 
     def step(self) -> float:
         t = time.perf_counter()
-        self.s.solve(max_iterations=1, tol=0.0, resume=True)
+        self.s.solve(max_iterations=1, tol=0.0, linear=self._linear, resume=True)
         return time.perf_counter() - t
-
-
-def cpu_sample(n_axial=3, steps=1, warmup=1):
-    """Seconds per oracle outer iteration on the short tube, and its node count."""
-    c = CpuCase(n_axial)
-    for _ in range(warmup):
-        c.step()
-    return float(np.mean([c.step() for _ in range(steps)])), c.n_nodes
 
 
 def cpu_spmv_gbs(indptr, indices, data, reps=3):
@@ -195,32 +226,54 @@ def cpu_spmv_gbs(indptr, indices, data, reps=3):
     return (132 * len(indices) + 72 * n + 8) / t / 1e9
 
 
+# the reference arm times at most this many full-size outer iterations (about 2 minutes each on
+# one host core), after one untimed iteration that also builds the first aggregation
+REFERENCE_MAX_STEPS = 2
+
+
 def reference_arm(args, rank, world):
-    """The reference's CPU algorithm (the oracle port) on the host cores, rank 0 only."""
+    """The reference's CPU path (the oracle's restatement, :class:`CpuCase`) on the full
+    400,686-node tube on the host cores, rank 0 only: measured outer iterations, no scaling."""
     if rank != 0:
         return
-    full_nodes = 400686
-    c = CpuCase(args.cpu_axial)
-    for _ in range(args.warmup):
+    t0 = time.perf_counter()
+    c = CpuCase(args.axial)
+    setup = time.perf_counter() - t0
+    warm = 1
+    for _ in range(warm):
         c.step()
-    times = [c.step() for _ in range(args.steps)]
-    n_nodes = c.n_nodes
-    per = float(np.mean(times)) * full_nodes / n_nodes
+    steps = max(1, min(args.steps, REFERENCE_MAX_STEPS))
+    times = [c.step() for _ in range(steps)]
+    per = float(np.mean(times))
     value = 1.0 / per
-    sample = (f"oracle outer iteration (NumPy assembly + SuperLU solve, the reference's CPU "
-              f"algorithm) on the same tube with {args.cpu_axial} axial cells ({n_nodes} nodes), "
-              f"time scaled linearly by node count to {full_nodes} nodes (a lower bound: the "
-              f"direct solve grows faster than linearly)")
+    host = host_info()
+    sample = (f"{steps} measured outer iterations of the full workload ({c.n_nodes:,} nodes) "
+              f"after {warm} untimed (of {args.steps} and {args.warmup} requested: each takes "
+              f"about two minutes on one core); NumPy assembly + ACM-FGMRES to 0.1; linear "
+              f"iterations {c.linear_iterations}; solver set-up {setup:.1f} s untimed")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+            "steps": steps, "warmup": warm, "steps_requested": args.steps,
+            "warmup_requested": args.warmup, "ms_per_step": per * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "precision": "fp64", "l2": "inputs larger than L2"},
+            "config": {"workload": WORKLOAD, "nodes": c.n_nodes, "precision": "fp64",
+                       "linear": "ACM-FGMRES (the reference's CPU AMG) to 0.1",
+                       "l2": "inputs larger than L2"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "host": host, "seconds": times},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(n_axial=3, steps=2):
+    """The bounded CPU sample of the default run (about 10-30 s): the reference arm's path on
+    the same tube shortened to ``n_axial`` cells, per outer iteration scaled linearly to the
+    full node count (assembly and the ACM cycle are linear in the nodes; the iteration counts
+    of the longer tube are not, so this is an estimate, the reference arm the measurement)."""
+    c = CpuCase(n_axial)
+    c.step()
+    return float(np.mean([c.step() for _ in range(steps)])), c.n_nodes, c.linear_iterations
 
 
 def bifurcation_workload(args):
@@ -364,6 +417,149 @@ def run_steps(solver, steps):
     return e0.elapsed_time(e1) / 1e3, recs
 
 
+def event_time(fn, reps=5):
+    """Mean seconds of ``fn`` on the current stream (CUDA events), after one untimed call."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+# ---------------------------------------------------------------- algorithmic bytes
+
+def spmv_bytes(n, nnz, value_bytes=8, vec_bytes=8):
+    """Block-CSR product: blocks, column indices, row pointers, x read once, y written."""
+    return (16 * value_bytes + 4) * nnz + 8 * (n + 1) + 2 * 4 * vec_bytes * n
+
+
+def gs_pass_bytes(n, nnz, value_bytes=8, vec_bytes=8):
+    """One Gauss-Seidel pass over all colours of a level: the level's blocks, indices and row
+    pointers once, each row's 4x4 inverse, b read, x read and written."""
+    return (16 * value_bytes + 4) * nnz + 8 * (n + 1) + 16 * value_bytes * n + 3 * 4 * vec_bytes * n
+
+
+def vcycle_bytes(stats, value_bytes=8, gs_levels=2, gs_passes=6, jacobi_sweeps=4,
+                 coarse_sweeps=8):
+    """Algorithmic bytes of one V-cycle over the hierarchy ``stats`` (rows and blocks per
+    level): Gauss-Seidel passes on the finest ``gs_levels`` (pre 1 + post 2 symmetric sweeps),
+    damped Jacobi sweeps below, the residual product, restriction and prolongation of each
+    level, and the permutations in and out of a Gauss-Seidel level's colour order."""
+    vb = value_bytes
+    total = 0
+    rows, blocks = stats["levels"], stats["blocks"]
+    for i, (n, nnz) in enumerate(zip(rows, blocks)):
+        last = i + 1 == len(rows)
+        vec = 4 * vb * n
+        if last and n <= 24:
+            total += 16 * n * n * vb + 2 * vec            # dense inverse times the vector
+            continue
+        if i < gs_levels:
+            total += gs_passes * gs_pass_bytes(n, nnz, vb, vb) + 4 * vec
+        else:
+            sweeps = coarse_sweeps if last else jacobi_sweeps
+            total += sweeps * (spmv_bytes(n, nnz, vb, vb) + 16 * vb * n + 2 * vec)
+        if not last:
+            total += spmv_bytes(n, nnz, vb, vb) + 3 * vec + 4 * n   # residual, restrict, prolong
+    return total
+
+
+def element_bytes(asm) -> dict:
+    """Algorithmic bytes of the element stage (the ideal of one pass over the data): the matrix
+    written once (128 B per block), b (32 B per node), the node values read once (188 B per node:
+    X 24, U 24, grad U 72, grad p 24, beta 24, d 8, s 8, own 4), and per element its
+    connectivity, mass flows and block positions. The colour-ordered scatter reads and writes
+    each element's n^2 blocks instead (``scatter``)."""
+    N, nnzb = asm.N, asm.nnzb
+    per_elem = sum(K.E * (4 * K.n + 8 * K.nip + 4 * K.n * K.n) for K in asm.kinds)
+    assemble = 128 * nnzb + 32 * N + 188 * N + per_elem
+    scatter = sum(K.E * K.n * K.n * 256 for K in asm.kinds)
+    # mass flows: X, U, grad p, P, d, s per node; mdot written; outflow, adv, vdiag
+    massflow = N * (24 + 24 + 24 + 8 + 8 + 8 + 24) + sum(K.E * (4 * K.n + 8 * K.nip)
+                                                         for K in asm.kinds)
+    return {"assemble": assemble, "assemble_scatter": scatter, "massflow": massflow}
+
+
+def stage_times(solver, peak, value_bytes=8):
+    """CUDA-event times and HBM fractions of the outer iteration's stages on the solver's
+    current state, and the Gauss-Seidel pass (the dominant kernel) alone; ``value_bytes`` is
+    the hierarchy's value size (8 FP64, 4 for the FP32 hierarchy)."""
+    import torch
+
+    from zvcfd_b200._lib import call, ptr, stream_ptr
+
+    asm = solver.asm
+    gradU, gradP, beta, diag = solver._stage1()
+    dnode, snode = solver.Vd / diag, solver.Vd / diag
+    own = solver._own_inflow()
+    vd = torch.zeros(solver.N, dtype=torch.float64, device="cuda")
+    mcopy = {k: v.clone() for k, v in solver.mdot.items()}
+    eb = element_bytes(asm)
+    out = {}
+    t = event_time(lambda: asm.assemble(solver.U, solver.mdot, gradU, beta, gradP, dnode, snode,
+                                        own=own))
+    out["assemble"] = {"ms": t * 1e3, "algorithmic_bytes": eb["assemble"],
+                       "frac": eb["assemble"] / t / 1e9 / peak,
+                       "scatter_bytes": eb["assemble_scatter"],
+                       "scatter_frac": eb["assemble_scatter"] / t / 1e9 / peak}
+    t = event_time(lambda: asm.massflow(solver.U, solver.P, gradP, dnode, snode, out=mcopy,
+                                        vdiag=vd))
+    out["massflow_vdiag"] = {"ms": t * 1e3, "algorithmic_bytes": eb["massflow"],
+                             "frac": eb["massflow"] / t / 1e9 / peak}
+    t = event_time(lambda: solver._assemble_fused())
+    out["assembly_stage"] = {"ms": t * 1e3, "what": "gradients, diagonal, limiter (frozen after "
+                                                    "10 iterations), assembly, boundary pass"}
+    A, b, _, x0 = solver._assemble_fused()
+    lin = solver.linear
+    lin.setup(A)
+    st = lin.stats()
+    r = b.reshape(-1) - A.matvec(x0)
+    t = event_time(lambda: lin.vcycle(r), reps=10)
+    vb = vcycle_bytes(st, value_bytes)
+    out["vcycle"] = {"ms": t * 1e3, "algorithmic_bytes": vb, "frac": vb / t / 1e9 / peak,
+                     "levels": st["levels"], "blocks": st["blocks"]}
+    n0, nnz0 = st["levels"][0], st["blocks"][0]
+    t = event_time(lambda: call("zvfv_solver_smooth", lin._h, 0, 1, stream_ptr()), reps=10)
+    gb = gs_pass_bytes(n0, nnz0, value_bytes, value_bytes)
+    kern = "double, double>" if value_bytes == 8 else "float, float>"
+    out["gs_pass"] = {"ms": t * 1e3, "algorithmic_bytes": gb, "frac": gb / t / 1e9 / peak,
+                      "kernel": "k_gs_colour_burst<16, " + ("4, " if value_bytes == 8 else "8, ")
+                                + kern,
+                      "launches": int(_gs_colours(lin))}
+    return out, st
+
+
+def _gs_colours(lin):
+    """Launches of one Gauss-Seidel pass on the finest level (its colours)."""
+    from zvcfd_b200._lib import call, lib, stream_ptr
+
+    before = lib.zvfv_launch_count()
+    call("zvfv_solver_smooth", lin._h, 0, 1, stream_ptr())
+    return lib.zvfv_launch_count() - before
+
+
+def iteration_bytes(solver, stats, linear_iterations, value_bytes=8):
+    """Algorithmic bytes of one outer iteration (mean over the timed window): the element
+    stage, two gradient passes, the boundary pass (matrix read and written once), per Krylov
+    step one V-cycle, one operator product and the Arnoldi passes (CGS2 over the basis, mean
+    index k), the update, and the hierarchy's coefficient refresh (Galerkin sums)."""
+    N, nnzb = solver.N, solver.nnzb
+    eb = element_bytes(solver.asm)
+    its = float(np.mean(linear_iterations)) if linear_iterations else 0.0
+    n4 = 4 * N * 8
+    krylov = vcycle_bytes(stats, value_bytes) + spmv_bytes(N, nnzb) + (4 * (its / 2 + 1) + 8) * n4
+    grad = 2 * (nnzb * (24 + 4) + 8 * N + 4 * 8 * N + 12 * 8 * N)
+    finalise = 2 * 128 * nnzb + 8 * nnzb + 4 * n4
+    refresh = sum(2 * 16 * 8 * nb for nb in stats["blocks"])
+    return eb["assemble"] + eb["massflow"] + grad + finalise + its * krylov + 2 * n4 + refresh
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,13 +570,14 @@ def main():
     ap.add_argument("--cpu-axial", type=int, default=3, help="axial cells of the CPU sample")
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-stages", action="store_true")
     ap.add_argument("--workload", default="tube", choices=["tube", "bifurcation", "ensemble"],
-                    help="tube: the headline (default); bifurcation: the ~2M-node transient "
-                         "Y-bifurcation; ensemble: 12 vessels solved together vs one by one")
+                    help="tube: the headline (default); bifurcation: config-2 transient; "
+                         "ensemble: config-4 batch")
     ap.add_argument("--nodes", type=int, default=2_000_000, help="bifurcation workload size")
     ap.add_argument("--instances", type=int, default=12, help="ensemble workload size")
     ap.add_argument("--max-nodes", type=int, default=1_200_000,
-                    help="ensemble workload: largest instance (log-uniform from 50,000)")
+                    help="largest ensemble instance")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark the timed steps with an NVTX range 'timed' (for ncu --nvtx-include)")
     args = ap.parse_args()
@@ -412,9 +609,13 @@ def main():
     from zvcfd_b200.solver import B200Solver
 
     m, fl, bcs = make_case(args.axial)
+    # two identical solvers: `value` is timed on one, `e2e` on the other over the same outer
+    # iterations (warm-up + 1 .. warm-up + steps) - the device work is deterministic
     solver = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1)
+    twin = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1)
     for _ in range(args.warmup):
         solver.iterate()
+        twin.iterate()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -432,47 +633,71 @@ def main():
         dist.barrier()
     per = elapsed / args.steps
     value = world * args.steps / elapsed
-    # end to end through the public API: host state in, one outer iteration, host state out
+    # end to end through the public API on the twin: every step copies the state in from
+    # pinned host memory, runs one outer iteration (B200Solver.iterate, whose record - the
+    # residuals, changes and flows - is read back) and copies the new state out
     N = m.n_nodes
     Uh = torch.empty((N, 3), dtype=torch.float64, pin_memory=True)
     Ph = torch.empty(N, dtype=torch.float64, pin_memory=True)
-    Uh.copy_(solver.U)
-    Ph.copy_(solver.P)
+    Uh.copy_(twin.U)
+    Ph.copy_(twin.P)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
+    twin_recs = []
     for _ in range(args.steps):
-        solver.U.copy_(Uh, non_blocking=True)
-        solver.P.copy_(Ph, non_blocking=True)
-        solver.iterate()
-        Uh.copy_(solver.U, non_blocking=True)
-        Ph.copy_(solver.P, non_blocking=True)
+        twin.U.copy_(Uh, non_blocking=True)
+        twin.P.copy_(Ph, non_blocking=True)
+        twin_recs.append(twin.iterate())
+        Uh.copy_(twin.U, non_blocking=True)
+        Ph.copy_(twin.P, non_blocking=True)
         torch.cuda.synchronize()
-    e2e = args.steps / (time.perf_counter() - t0) * world
-    # mixed precision on the same case
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        e2e_s = max_over_ranks(e2e_s, dist, "cuda")
+    e2e = world * args.steps / e2e_s
+    same = [r["linear_iterations"] for r in recs] == [r["linear_iterations"] for r in twin_recs]
+    twin.close()
+    # mixed precision on the same case and window
     mixed = B200Solver(m, fl, bcs, linear="b200-mixed", linear_rtol=0.1)
     for _ in range(args.warmup):
         mixed.iterate()
     melapsed, mrecs = run_steps(mixed, args.steps)
     extra = {"fp64_linear_iterations": [r["linear_iterations"] for r in recs],
+             "e2e_window_matches_value_window": same,
              "mixed": {"ms_per_step": melapsed / args.steps * 1e3,
                        "outer_iterations_per_s": args.steps / melapsed,
                        "speedup_vs_fp64": elapsed / melapsed,
                        "linear_iterations": [r["linear_iterations"] for r in mrecs]}}
-    # SpMV roofline on the assembled matrix
-    sp, n, nnzb = spmv_roofline(solver)
     peak, peak_kind = peaks()
-    roof = {"kernel": "k_bsr_spmv<16> fp64", "bound": "hbm", "achieved": sp["fp64"]["gbs"],
-            "peak": peak, "unit": "GB/s", "frac": sp["fp64"]["gbs"] / peak,
-            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-            else "fallback 6.65 TB/s",
-            "algorithmic_bytes": sp["fp64"]["bytes"],
-            "traffic": SPMV_TRAFFIC_PER_ALGORITHMIC_BYTE * sp["fp64"]["bytes"],
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel "
-                              "on the 211,551-node tube (5,214,011 blocks, larger than L2), scaled "
-                              "by algorithmic bytes (profiles/k_bsr_spmv_fp64_curved_tube.txt)"}
+    peak_source = (f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                   else "fallback 6.65 TB/s")
+    # SpMV on the assembled matrix, stages, the dominant kernel alone
+    sp, n, nnzb = spmv_roofline(solver)
     extra["spmv"] = {"fp64_gbs": sp["fp64"]["gbs"], "fp32_gbs": sp["fp32"]["gbs"],
                      "fp64_us": sp["fp64"]["seconds"] * 1e6, "fp32_us": sp["fp32"]["seconds"] * 1e6,
-                     "nnzb": nnzb, "rows": n}
+                     "fp64_frac": sp["fp64"]["gbs"] / peak, "nnzb": nnzb, "rows": n}
+    roof = None
+    if not args.no_stages:
+        stages, hstats = stage_times(solver, peak)
+        mstages, _ = stage_times(mixed, peak, 4)
+        ib = iteration_bytes(solver, hstats, extra["fp64_linear_iterations"])
+        extra["stages"] = {"fp64": stages,
+                           "mixed": {k: mstages[k] for k in ("vcycle", "gs_pass")}}
+        extra["outer_iteration_roofline"] = {
+            "algorithmic_bytes": ib, "achieved_gbs": ib / per / 1e9, "peak": peak,
+            "frac": ib / per / 1e9 / peak, "unit": "GB/s",
+            "note": "sum of the algorithmic bytes of every stage of one outer iteration "
+                    "(mean Krylov steps of the window) over ms_per_step"}
+        g = stages["gs_pass"]
+        roof = {"kernel": g["kernel"] + " (one pass over all colours of the finest level)",
+                "bound": "hbm", "achieved": g["algorithmic_bytes"] / (g["ms"] * 1e-3) / 1e9,
+                "peak": peak, "unit": "GB/s", "frac": g["frac"], "peak_source": peak_source,
+                "algorithmic_bytes": g["algorithmic_bytes"],
+                "traffic": None if GS_TRAFFIC_PER_ALGORITHMIC_BYTE is None
+                else GS_TRAFFIC_PER_ALGORITHMIC_BYTE * g["algorithmic_bytes"],
+                "traffic_source": GS_TRAFFIC_SOURCE}
     if not args.no_converge and rank == 0:
         conv = {}
         for tag, lin in (("fp64", "b200"), ("mixed", "b200-mixed")):
@@ -490,20 +715,23 @@ def main():
         conv["mixed"]["field_error_vs_fp64"] = {
             "U": float(np.linalg.norm(fmx["U"] - f64["U"]) / np.linalg.norm(f64["U"])),
             "P": float(np.linalg.norm(fmx["P"] - f64["P"]) / np.linalg.norm(f64["P"]))}
+        conv["mixed"]["speedup_vs_fp64"] = conv["fp64"]["seconds"] / conv["mixed"]["seconds"]
         extra["to_1e-8"] = conv
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        t_cpu, n_cpu = cpu_sample(args.cpu_axial)
+        t_cpu, n_cpu, its = cpu_baseline_sample(args.cpu_axial)
         per_cpu = t_cpu * N / n_cpu
         A, _, _, _ = solver._assemble_fused()
         gbs = cpu_spmv_gbs(A.indptr.cpu().numpy(), A.indices.cpu().numpy(),
                            A.data.cpu().numpy())
         cpu = {"value": 1.0 / per_cpu, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"oracle outer iteration (NumPy assembly + SuperLU) on the same tube "
-                         f"with {args.cpu_axial} axial cells ({n_cpu} nodes), scaled linearly by "
-                         f"node count (a lower bound); SciPy BSR SpMV on the full matrix: "
+               "sample": f"the reference arm's path (oracle NumPy assembly + ACM-FGMRES to 0.1) "
+                         f"on the same tube cross-section with {args.cpu_axial} axial cells "
+                         f"({n_cpu} nodes, linear iterations {its}), per outer iteration scaled "
+                         f"by node count to {N:,} nodes: an estimate (bench.py --impl reference "
+                         f"measures the full size); SciPy BSR SpMV on the full matrix "
                          f"{gbs:.2f} GB/s",
-               "spmv_gbs": gbs}
+               "spmv_gbs": gbs, "host": host_info()}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,

@@ -258,6 +258,10 @@ int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, i
                         double *residual, int *converged, void *stream);
 /* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:905-918) */
 int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
+/* `passes` forward multicolour Gauss-Seidel passes on level `level` (a Gauss-Seidel level)
+ * over that level's own work vectors: the smoother kernel alone, for timing (no reference
+ * counterpart: AmgX's smoother is internal to its V-cycle). */
+int zvfv_solver_smooth(void *handle, int level, int passes, void *stream);
 /* Hierarchy options beyond create (each takes effect at the next set-up, which rebuilds):
  *   "autotune" (0/1, default 0): after each rebuild, every level of 2048 rows or more times one
  *       smoothing pass at 8, 16 and 32 lanes per row and keeps the fastest (AmgX fixes its

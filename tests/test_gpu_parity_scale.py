@@ -1,0 +1,60 @@
+"""Converged-field parity beyond the toy meshes.
+
+- A mid-size curved Carreau-Yasuda tube (the headline tube's geometry and fluid, about 6k
+  nodes, hexahedral core and three wedge wall layers) against the reference's own CPU solver
+  (``curved_mid.npz``: ``ReferenceSolver`` with lagged Rhie-Chow and a SuperLU solve of every
+  linearisation, ``zvcfd/fv/reference.py:952-980``), in FP64 and with the FP32 hierarchy:
+  relative L2 <= 1e-8.
+- The plain FP64 Poiseuille pipe at its full 49,977 nodes against the oracle's converged fields
+  (``c0_pipe.npz``: the oracle's restatement of the same solver with its ACM-FGMRES, since the
+  reference's direct solve does not finish at this size): relative L2 <= 1e-8.
+"""
+
+import numpy as np
+import pytest
+
+from fixtures import fluid_of, load, mesh_of, pipe_bcs
+
+pytestmark = pytest.mark.gpu
+
+
+def _close(f, U, P):
+    assert np.linalg.norm(f["U"] - U) <= 1e-8 * np.linalg.norm(U)
+    assert np.linalg.norm(f["P"] - P) <= 1e-8 * np.linalg.norm(P - P.mean()) + 1e-9 * np.ptp(P)
+    np.testing.assert_allclose(f["U"], U, atol=1e-8 * np.abs(U).max())
+    np.testing.assert_allclose(f["P"], P, atol=1e-8 * np.ptp(P))
+
+
+@pytest.mark.parametrize("linear", ["b200", "b200-mixed"])
+def test_mid_size_curved_tube_matches_reference(linear):
+    from zvcfd_b200.solver import B200Solver
+
+    g = load("curved_mid")
+    m = mesh_of(g)
+    assert m.n_nodes > 5000
+    s = B200Solver(m, fluid_of(g), pipe_bcs("curved_mid", g, m), advection=1.0, linear=linear)
+    rep = s.solve(max_iterations=800, tol=1e-11)
+    assert rep["converged"], rep["history"][-1]
+    _close(s.fields(), g["U"], g["P"])
+    assert abs(rep["history"][-1]["imbalance"]) < 1e-11
+    s.close()
+
+
+@pytest.mark.parametrize("linear", ["b200", "b200-mixed"])
+def test_config0_pipe_matches_the_oracle(linear):
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    from make_oracle_golden import c0_case
+    from zvcfd_b200.solver import B200Solver
+
+    g = load("c0_pipe")
+    m, fl, bcs = c0_case()
+    assert m.n_nodes == int(g["n_nodes"]) == 49977
+    assert float(np.abs(m.nodes).sum()) == float(g["node_checksum"])
+    s = B200Solver(m, fl, bcs, advection=1.0, linear=linear, linear_rtol=0.1)
+    rep = s.solve(max_iterations=800, tol=1e-11)
+    assert rep["converged"], rep["history"][-1]
+    _close(s.fields(), g["U"], g["P"])
+    s.close()

@@ -38,6 +38,12 @@ namespace {
 
 constexpr int CTA_WARPS = 4;
 constexpr int CTA_THREADS = CTA_WARPS * 32;
+// Resident CTAs per SM the per-iteration kernels are compiled for: a register cap of 128. The
+// kernels are latency-bound; uncapped (160-200 registers) only two or three CTAs fit on an SM,
+// and four measured fastest (assembly on the 400k-node tube 6.6 ms uncapped, 4.7 ms at four).
+#ifndef ZV_ELEMENT_MIN_CTAS
+#define ZV_ELEMENT_MIN_CTAS 4
+#endif
 
 template <int K>
 struct Team {
@@ -212,6 +218,11 @@ __device__ inline void prefetch_block(const double *p) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], 128;" ::"l"(p) : "memory");
 }
 
+// One 128-byte line of node data towards L2 (the next element's gathers).
+__device__ inline void prefetch_line(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p) : "memory");
+}
+
 // Team coordinates of this thread inside the grid-stride walk.
 template <int K>
 struct Walk {
@@ -314,9 +325,10 @@ k_geobuild(const int *__restrict__ conn, const double *__restrict__ Xn, long lon
         if (on && wk.lane < T::N) {
             const int a = wk.lane;
             double v = 0.0;
-            for (int i = 0; i < MAXI; ++i) {
+#pragma unroll
+            for (int i = 0; i < T::MAXF; ++i) {
                 const int s = tb.ips[a][i];
-                if (s < 0) break;
+                if (s < 0) continue;
                 double f = 0.0;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) f += (st.xs[k][s] - st.X[a][k]) * st.A[k][s];
@@ -383,9 +395,10 @@ k_statics(const int *__restrict__ conn, long long base, long long count,
         if (on && wk.lane < N) {
             const int a = wk.lane;
             double v = 0.0, dv = 0.0;
-            for (int i = 0; i < MAXI; ++i) {
+#pragma unroll
+            for (int i = 0; i < T::MAXF; ++i) {
                 const int s = tb.ips[a][i];
-                if (s < 0) break;
+                if (s < 0) continue;
                 const double A[3] = {st.A[0][s], st.A[1][s], st.A[2][s]};
                 double Ji[9];
 #pragma unroll
@@ -448,7 +461,7 @@ struct DiagStage {
 // The momentum diagonal a_P: per flux point the viscous coefficient of each edge node on its
 // own row and the upwind part of the mass flow (zvcfd/fv/reference.py:694-724).
 template <int K, bool STORED>
-__global__ void __launch_bounds__(CTA_THREADS)
+__global__ void __launch_bounds__(CTA_THREADS, ZV_ELEMENT_MIN_CTAS)
 k_diag(const DiagArgs g, long long base, long long count) {
     using T = Topo<K>;
     constexpr int N = T::N;
@@ -501,9 +514,10 @@ k_diag(const DiagArgs g, long long base, long long count) {
         if (on && wk.lane < N) {
             const int a = wk.lane;
             double d = 0.0;
-            for (int i = 0; i < MAXI; ++i) {
+#pragma unroll
+            for (int i = 0; i < T::MAXF; ++i) {
                 const int s = tb.ips[a][i];
-                if (s < 0) break;
+                if (s < 0) continue;
                 d += tb.sgn[a][i] > 0 ? st.ca[s] : st.cb[s];
             }
             g.out[st.node[a]] += d;
@@ -584,7 +598,7 @@ __device__ inline double2 block_entries(const double (*P)[L], int j, int q, doub
 // except on an own inflow node's row for the faces it is upwind of; continuity -sg (rho d
 // (N(s) grad p) . A + the transient Rhie-Chow part).
 template <int K, bool STORED>
-__global__ void __launch_bounds__(CTA_THREADS)
+__global__ void __launch_bounds__(CTA_THREADS, ZV_ELEMENT_MIN_CTAS)
 k_assemble(const AsmArgs g, long long base, long long count) {
     using T = Topo<K>;
     using TM = Team<K>;
@@ -595,17 +609,30 @@ k_assemble(const AsmArgs g, long long base, long long count) {
     Walk<K> wk;
     AsmStage<K> &st = st_all[wk.slot_in_cta()];
     const int lane = wk.lane;
+    constexpr int PPL = (NN + L - 1) / L;                  // block positions per lane
     for (long long e0 = wk.first; e0 < count; e0 += wk.stride) {
         const long long le = e0 + wk.team;
         const bool on = le < count;
         const long long slot = base + le;
         const double *rec = g.geo + (STORED ? slot * T::REC : 0);
+        // the next element of this team: its nodes and block positions, read now so that its
+        // node data and blocks can be sent towards L2 while this element is worked on
+        const long long nle = le + wk.stride;
+        const bool next_on = nle < count;
+        const long long nslot = base + nle;
+        int next_node = -1, next_pos[PPL];
+        if (next_on && lane < N) next_node = __ldg(g.conn + nslot * N + lane);
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) {
+            const int p = j * L + lane;
+            next_pos[j] = next_on && p < NN ? __ldg(g.pos + nslot * NN + p) : -1;
+        }
         // ---- node lanes: stage the element's node values; every lane: block positions
         if (on) {
             for (int p = lane; p < NN; p += L) {
                 const int q = __ldg(g.pos + slot * NN + p);
                 st.pos[p] = q;
-                if (q >= 0) prefetch_block(g.data + (long long)q * 16);
+                if (q >= 0 && e0 == wk.first) prefetch_block(g.data + (long long)q * 16);
             }
         }
         if (on && lane < N) {
@@ -689,6 +716,27 @@ k_assemble(const AsmArgs g, long long base, long long count) {
             st.d[s] = d;
         }
         __syncwarp();
+        // ---- the next element's node data, mass flows and blocks towards L2
+        if (next_node >= 0) {
+            const long long n = next_node;
+            prefetch_line(g.X + n * 3);
+            prefetch_line(g.U + n * 3);
+            prefetch_line(g.gradP + n * 3);
+            prefetch_line(g.dnode + n);
+            prefetch_line(g.snode + n);
+            prefetch_line(g.own + n);
+            if (!g.stokes) {
+                prefetch_line(g.gradU + n * 9);
+                prefetch_line(g.gradU + n * 9 + 8);
+                prefetch_line(g.beta + n * 3);
+            }
+            if (g.nlev > 0) prefetch_line(g.Uo1 + n * 3);
+            if (g.nlev > 1) prefetch_line(g.Uo2 + n * 3);
+        }
+        if (next_on && lane < NIP) prefetch_line(g.mdot + nslot * NIP + lane);
+#pragma unroll
+        for (int j = 0; j < PPL; ++j)
+            if (next_pos[j] >= 0) prefetch_block(g.data + (long long)next_pos[j] * 16);
         // ---- pair lanes, then store lanes, one round of L pairs at a time
 #pragma unroll 1
         for (int round = 0; round < TM::PAIR_ROUNDS; ++round) {
@@ -698,9 +746,10 @@ k_assemble(const AsmArgs g, long long base, long long count) {
                 double dg = 0.0, rcd = 0.0, pv[3] = {0.0, 0.0, 0.0}, tr[9];
 #pragma unroll
                 for (int i = 0; i < 9; ++i) tr[i] = 0.0;
-                for (int i = 0; i < MAXI; ++i) {
+#pragma unroll
+                for (int i = 0; i < T::MAXF; ++i) {
                     const int s = tb.ips[a][i];
-                    if (s < 0) break;
+                    if (s < 0) continue;
                     const double sg = (double)tb.sgn[a][i];
                     const double A[3] = {st.A[0][s], st.A[1][s], st.A[2][s]};
                     double Ji[9], G[3];
@@ -764,9 +813,10 @@ k_assemble(const AsmArgs g, long long base, long long count) {
             const int a = lane >> 2, k = lane & 3;
             const bool keep_out = k < 3 && st.own[a];
             double r = 0.0;
-            for (int i = 0; i < MAXI; ++i) {
+#pragma unroll
+            for (int i = 0; i < T::MAXF; ++i) {
                 const int s = tb.ips[a][i];
-                if (s < 0) break;
+                if (s < 0) continue;
                 if (keep_out && (st.m[s] >= 0 ? tb.ia[s] : tb.ib[s]) == a) continue;
                 r -= tb.sgn[a][i] * st.R[k][s];
             }
@@ -809,7 +859,7 @@ struct MassStage {
 // (zvcfd/fv/reference.py:922-948). With VDIAG the flux lanes also form the viscous terms of
 // the next diagonal from the same velocity, which then needs no element pass of its own.
 template <int K, bool STORED, bool VDIAG>
-__global__ void __launch_bounds__(CTA_THREADS)
+__global__ void __launch_bounds__(CTA_THREADS, ZV_ELEMENT_MIN_CTAS)
 k_massflow(const MassArgs g, long long base, long long count) {
     using T = Topo<K>;
     constexpr int N = T::N, NIP = T::NIP;
@@ -824,6 +874,8 @@ k_massflow(const MassArgs g, long long base, long long count) {
         const bool on = le < count;
         const long long slot = base + le;
         const double *rec = g.geo + (STORED ? slot * T::REC : 0);
+        const long long nle = le + wk.stride;              // this team's next element
+        const int next_node = nle < count && lane < N ? __ldg(g.conn + (base + nle) * N + lane) : -1;
         if (on && lane < N) {
             const int a = lane;
             const long long n = __ldg(g.conn + slot * N + a);
@@ -886,13 +938,25 @@ k_massflow(const MassArgs g, long long base, long long count) {
                 st.vb[s] = -viscous_coefficient<K>(tb, ib, s, Ji, A, mu, g.transpose);
             }
         }
+        if (next_node >= 0) {
+            const long long n = next_node;
+            prefetch_line(g.X + n * 3);
+            prefetch_line(g.U + n * 3);
+            prefetch_line(g.gradP + n * 3);
+            prefetch_line(g.P + n);
+            prefetch_line(g.dnode + n);
+            prefetch_line(g.snode + n);
+            if (g.nlev > 0) prefetch_line(g.Uo1 + n * 3);
+            if (g.nlev > 1) prefetch_line(g.Uo2 + n * 3);
+        }
         __syncwarp();
         if (on && lane < N) {
             const int a = lane;
             double out = 0.0, ad = 0.0, vd = 0.0;
-            for (int i = 0; i < MAXI; ++i) {
+#pragma unroll
+            for (int i = 0; i < T::MAXF; ++i) {
                 const int s = tb.ips[a][i];
-                if (s < 0) break;
+                if (s < 0) continue;
                 const double m = st.m[s];
                 if (tb.sgn[a][i] > 0) {
                     out += m;
@@ -975,9 +1039,10 @@ k_limiter(const int *__restrict__ conn, long long base, long long count,
             const double u = __ldg(U + n * 3 + k);
             const double up = __ldg(hi + n * 3 + k) - u, down = __ldg(lo + n * 3 + k) - u;
             double f = beta[n * 3 + k];
-            for (int i = 0; i < MAXI; ++i) {
+#pragma unroll
+            for (int i = 0; i < T::MAXF; ++i) {
                 const int s = tb.ips[a][i];
-                if (s < 0) break;
+                if (s < 0) continue;
                 const double delta = g0 * (st.xs[0][s] - st.X[a][0]) + g1 * (st.xs[1][s] - st.X[a][1]) +
                                      g2 * (st.xs[2][s] - st.X[a][2]);
                 if (fabs(delta) > 1e-300)

@@ -850,6 +850,24 @@ void jacobi_t(int lanes, long long n, const Level &v, const V *data, const V *di
     }
 }
 
+// A launch of 256-thread CTAs that may begin while the previous kernel in the stream is still
+// draining (Programmatic Dependent Launch): the kernel must wait (griddepcontrol.wait) before it
+// touches anything that kernel writes. Captured into a CUDA graph as a programmatic edge.
+template <typename... P, typename... A>
+void launch_dependent(void (*kern)(P...), unsigned grid, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<P>(args)...);
+}
+
 // one Gauss-Seidel pass over the colours of level v, forward or backward: on the colour-ordered
 // copy (data, dinv, b, x colour-ordered; each colour a contiguous row range), or with TRANS on
 // A^T in the original numbering (columns of A through the transpose structure, D^-T)
@@ -869,9 +887,10 @@ void gs_pass(const Level &v, const V *data, const V *dinv, const T *b, T *x, T o
             else if (G == 16) k_gs_colour_t<16, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
             else k_gs_colour_t<32, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
         } else {
-            if (G == 8) k_gs_colour<8, true, V, T><<<grid, 256, 0, st>>>(cnt, o, nullptr, v.pptr, v.pidx, data, dinv, b, x, omega);
-            else if (G == 16) k_gs_colour<16, true, V, T><<<grid, 256, 0, st>>>(cnt, o, nullptr, v.pptr, v.pidx, data, dinv, b, x, omega);
-            else k_gs_colour<32, true, V, T><<<grid, 256, 0, st>>>(cnt, o, nullptr, v.pptr, v.pidx, data, dinv, b, x, omega);
+            constexpr int D = gs_prefetch_depth<V>();
+            if (G == 8) launch_dependent(k_gs_colour_pdl<8, 2 * D, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
+            else if (G == 16) launch_dependent(k_gs_colour_pdl<16, D, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
+            else launch_dependent(k_gs_colour_pdl<32, (D + 1) / 2, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
         }
         count_launch();
     }
@@ -1347,6 +1366,33 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream) {
     s->st = as_stream(stream);
     s->H.st = s->st;
     return s->precondition(r, z);
+}
+
+// `passes` forward Gauss-Seidel passes over the colours of level `level` (one of the
+// Gauss-Seidel levels) on the level's own work vectors, in the hierarchy's precision: the
+// smoother kernel alone, for timing it (the V-cycle graph runs the same launches).
+int zvfv_solver_smooth(void *handle, int level, int passes, void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || !s->data || level < 0 || level >= (int)s->H.L.size() || passes < 1) {
+        set_error("solver_smooth: not set up, or no level %d", level);
+        return BAD_ARGUMENT;
+    }
+    Level &v = s->H.L[level];
+    if (v.gs_off.empty() || !v.pb || !v.x2) {
+        set_error("solver_smooth: level %d is not smoothed by Gauss-Seidel", level);
+        return BAD_ARGUMENT;
+    }
+    const cudaStream_t st = as_stream(stream);
+    for (int q = 0; q < passes; ++q) {
+        if (s->H.prm.precision == 1)
+            gs_pass<false, float, float>(v, v.pdata32, v.pdinv32, static_cast<const float *>(v.pb),
+                                         static_cast<float *>(v.x2), (float)s->H.prm.omega, false, st);
+        else
+            gs_pass<false, double, double>(v, v.pdata64, v.pdinv64,
+                                           static_cast<const double *>(v.pb),
+                                           static_cast<double *>(v.x2), s->H.prm.omega, false, st);
+    }
+    return launch_status("solver_smooth");
 }
 
 // levels, and per level rows and blocks (arrays of max_levels entries)

@@ -256,6 +256,7 @@ def header_source() -> str:
         out.append(f"    static constexpr int CONSTG = {int(t.const_gradient)};")
         out.append(f"    static constexpr int NG = {t.n_grad};")
         out.append(f"    static constexpr int REC = {t.record_doubles};")
+        out.append(f"    static constexpr int MAXF = {int((t.node_ips >= 0).sum(1).max())};")
         out.append(f"    __device__ static const int (*edge())[2] {{ return k{K}_EDGE; }}")
         out.append(f"    __device__ static const int (*mask())[3] {{ return k{K}_MASK; }}")
         out.append(f"    __device__ static const double (*nt())[{t.n_ip}] {{ return k{K}_NT; }}")
