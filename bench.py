@@ -44,12 +44,18 @@ GS_TRAFFIC_PER_ALGORITHMIC_BYTE = None
 GS_TRAFFIC_SOURCE = None
 
 
-def make_case(n_axial=285):
+FULL_AXIAL = 285          # axial cells of the full 90-degree tube
+
+
+def make_case(n_axial=FULL_AXIAL, same_cells=False):
+    """The tube with ``n_axial`` cells over its 90-degree bend, or with ``same_cells`` a shorter
+    arc of the full tube's cells (the bend angle scaled with ``n_axial``)."""
     from zvcfd_b200.fluid import CarreauYasuda, Fluid
     from zvcfd_b200.mesh import curved_tube
 
     R = 2e-3
-    m = curved_tube(R, 20e-3, np.pi / 2, n_core=20, n_ring=12, n_axial=n_axial, layers=5,
+    angle = np.pi / 2 * (n_axial / FULL_AXIAL if same_cells else 1.0)
+    m = curved_tube(R, 20e-3, angle, n_core=20, n_ring=12, n_axial=n_axial, layers=5,
                     growth=0.8)
     z = {zz.name: k for k, zz in m.zones.items()}
 
@@ -186,11 +192,11 @@ class CpuCase:
     passes, aggregates kept for 10 set-ups, restart 30), as SuperLU does not finish at this
     size. NumPy's element-wise and SciPy's sparse kernels run on one thread."""
 
-    def __init__(self, n_axial=285):
+    def __init__(self, n_axial=FULL_AXIAL):
         from oracle.fv import OracleSolver
         from oracle.linear import ACM, pairwise_arrays
 
-        m, fl, bcs = make_case(n_axial)
+        m, fl, bcs = make_case(n_axial, same_cells=True)
         self.n_nodes = m.n_nodes
         self.s = OracleSolver(m, fl, bcs)
         self.acm = ACM(coarse=400, matcher=pairwise_arrays, rebuild_every=10)
@@ -266,11 +272,12 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_sample(n_axial=3, steps=2):
+def cpu_baseline_sample(n_axial=6, steps=2):
     """The bounded CPU sample of the default run (about 10-30 s): the reference arm's path on
-    the same tube shortened to ``n_axial`` cells, per outer iteration scaled linearly to the
-    full node count (assembly and the ACM cycle are linear in the nodes; the iteration counts
-    of the longer tube are not, so this is an estimate, the reference arm the measurement)."""
+    a short arc of the same tube (``n_axial`` of its cells, the same cell shapes), per outer
+    iteration scaled linearly to the full node count (assembly and the ACM cycle are linear in
+    the nodes; the iteration counts of the longer tube are not, so this is an estimate, the
+    reference arm the measurement)."""
     c = CpuCase(n_axial)
     c.step()
     return float(np.mean([c.step() for _ in range(steps)])), c.n_nodes, c.linear_iterations
@@ -529,7 +536,7 @@ def stage_times(solver, peak, value_bytes=8):
     gb = gs_pass_bytes(n0, nnz0, value_bytes, value_bytes)
     kern = "double, double>" if value_bytes == 8 else "float, float>"
     out["gs_pass"] = {"ms": t * 1e3, "algorithmic_bytes": gb, "frac": gb / t / 1e9 / peak,
-                      "kernel": "k_gs_colour_burst<16, " + ("4, " if value_bytes == 8 else "8, ")
+                      "kernel": "k_gs_colour_pdl<16, " + ("4, " if value_bytes == 8 else "8, ")
                                 + kern,
                       "launches": int(_gs_colours(lin))}
     return out, st
@@ -567,7 +574,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--axial", type=int, default=285, help="axial cells (285: the full tube)")
-    ap.add_argument("--cpu-axial", type=int, default=3, help="axial cells of the CPU sample")
+    ap.add_argument("--cpu-axial", type=int, default=6,
+                    help="axial cells of the CPU sample (an arc of the full tube's cells)")
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stages", action="store_true")
@@ -726,7 +734,7 @@ def main():
                            A.data.cpu().numpy())
         cpu = {"value": 1.0 / per_cpu, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"the reference arm's path (oracle NumPy assembly + ACM-FGMRES to 0.1) "
-                         f"on the same tube cross-section with {args.cpu_axial} axial cells "
+                         f"on a {args.cpu_axial}-cell arc of the same tube (the same cells) "
                          f"({n_cpu} nodes, linear iterations {its}), per outer iteration scaled "
                          f"by node count to {N:,} nodes: an estimate (bench.py --impl reference "
                          f"measures the full size); SciPy BSR SpMV on the full matrix "

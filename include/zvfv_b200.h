@@ -258,6 +258,10 @@ int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, i
                         double *residual, int *converged, void *stream);
 /* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:905-918) */
 int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
+/* z = one V-cycle of the transposed hierarchy applied to r (A^T, D^-T, transposed Gauss-Seidel
+ * sweeps, the dense coarsest inverse transposed on every level): the preconditioner of the
+ * parameter adjoint's FGMRES; no reference counterpart (the reference has no adjoint) */
+int zvfv_solver_vcycle_t(void *handle, const double *r, double *z, void *stream);
 /* `passes` forward multicolour Gauss-Seidel passes on level `level` (a Gauss-Seidel level)
  * over that level's own work vectors: the smoother kernel alone, for timing (no reference
  * counterpart: AmgX's smoother is internal to its V-cycle). */

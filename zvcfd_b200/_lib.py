@@ -59,6 +59,7 @@ _SIGNATURES = {
     "zvfv_bsr_spmv_t": ([I64, P, P, P, P, P, P, I32, P], None),
     "zvfv_solver_create": ([P, I32, I32, I32, I32, I32, I32, F64, I32, I32, I32, I32], None),
     "zvfv_solver_smooth": ([P, I32, I32, P], None),
+    "zvfv_solver_vcycle_t": ([P, P, P, P], None),
     "zvfv_solver_setup": ([P, I64, I64, P, P, P, P], None),
     "zvfv_solver_solve": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_solve_t": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),

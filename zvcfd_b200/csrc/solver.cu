@@ -1368,6 +1368,21 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream) {
     return s->precondition(r, z);
 }
 
+// z = one transposed V-cycle applied to r: the hierarchy of A on every level's transpose
+// (A^T, D^-T, transposed Gauss-Seidel sweeps, the dense inverse transposed), the
+// preconditioner of adjoint solves outside this library. Builds the transposes on first use.
+int zvfv_solver_vcycle_t(void *handle, const double *r, double *z, void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || !s->data) {
+        set_error("solver_vcycle_t: not set up");
+        return BAD_ARGUMENT;
+    }
+    s->st = as_stream(stream);
+    s->H.st = s->st;
+    ZV_TRY(s->H.ensure_transpose());
+    return s->precondition(r, z, true);
+}
+
 // `passes` forward Gauss-Seidel passes over the colours of level `level` (one of the
 // Gauss-Seidel levels) on the level's own work vectors, in the hierarchy's precision: the
 // smoother kernel alone, for timing it (the V-cycle graph runs the same launches).
