@@ -58,7 +58,7 @@ def _solve(theta, start=None):
     s = B200Solver(m, fl, bcs, advection=1.0, linear_rtol=0.1)
     if start is not None:
         s.initialise(U=start[0], P=start[1])
-    rep = s.solve(max_iterations=1500, tol=1e-13)
+    rep = s.solve(max_iterations=1500, tol=1e-12)
     assert rep["converged"], rep["history"][-1]
     return SteadyResidual(s, z["inlet"], [z["outlet1"], z["outlet2"]], _walls(m, z))
 

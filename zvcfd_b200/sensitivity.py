@@ -20,8 +20,8 @@ stress per wall part) as torch functions of ``(z, theta)``, element type by elem
 that every transposed Jacobian product ``(dR/dz)^T v`` is one reverse pass through them. The
 adjoint system is solved by restarted FGMRES whose preconditioner is the transposed V-cycle of
 the AMG hierarchy the forward solve built for its last linearisation (``zvfv_solver_vcycle_t``:
-``A^T``, ``D^-T`` and transposed Gauss-Seidel sweeps on every level) for the ``x`` block and the
-identity for the mass flows. The reference has no adjoint; the forward state, boundary data and
+``A^T``, ``D^-T`` and transposed Gauss-Seidel sweeps on every level) for the ``x`` block, with
+the mass-flow rows' coupling to ``x`` applied exactly (a block-triangular preconditioner). The reference has no adjoint; the forward state, boundary data and
 hierarchy are the device solver's own.
 
 Parameters ``theta``: the inlet flow rate, per lumped outlet ``(Rp, C, Rd)`` and the fluid's
@@ -43,10 +43,19 @@ def _carreau_yasuda(rate, mu0, muinf, lam, a, n):
     return muinf + (mu0 - muinf) * (1.0 + (lam * rate) ** a) ** ((n - 1.0) / a)
 
 
+def _sqrt0(v):
+    """``sqrt(v)`` with a zero derivative where ``v = 0`` (a flux point inside an element whose
+    nodes all lie on a no-slip wall has no shear; there the viscosity's slope in the shear rate
+    is zero, while sqrt's derivative would be infinite and turn the reverse pass into NaN)."""
+    pos = v > 0
+    return torch.where(pos, torch.sqrt(torch.where(pos, v, torch.ones_like(v))),
+                       torch.zeros_like(v))
+
+
 def _rate(L):
     """Shear rate ``sqrt(2 D:D)`` of velocity gradients ``L (..., 3, 3)``."""
     D = 0.5 * (L + L.transpose(-1, -2))
-    return torch.sqrt(2.0 * (D * D).sum((-1, -2)))
+    return _sqrt0(2.0 * (D * D).sum((-1, -2)))
 
 
 class _KindGeometry:
@@ -243,7 +252,7 @@ class SteadyResidual:
             q_z = (self.s._flow_W[k] @ mb + self.s._flow_c[k]) / self.rho
             out.append(q_z / theta[0])
         tau = self.wall_shear(x[:, :3], theta[-1])
-        mag = torch.sqrt((tau * tau).sum(1) + 1e-300)
+        mag = _sqrt0((tau * tau).sum(1))
         for name, nodes in self.walls.items():
             a = self.wall.node_area[nodes]
             out.append((mag[nodes] * a).sum() / a.sum())
@@ -257,7 +266,7 @@ class SteadyResidual:
         Uq = U[torch.where(on, elem, torch.zeros_like(elem))] * on[..., None]
         L = torch.einsum("qaj,qak->qjk", Uq, w.G)
         D = L + L.transpose(1, 2)
-        rate = torch.sqrt(0.5 * (D * D).sum((1, 2)))
+        rate = _sqrt0(0.5 * (D * D).sum((1, 2)))
         mu = self._mu(rate, mu0)
         t = mu[:, None] * torch.einsum("qjk,qk->qj", D, w.nrm)
         tn = (t * w.nrm).sum(1, keepdim=True)
@@ -278,7 +287,7 @@ class SteadyResidual:
         call("zvfv_solver_vcycle_t", lin._h, ptr(vx), ptr(out), stream_ptr())
         return out * self.s.rs
 
-    def adjoint(self, gx, gm, x, mdot, theta, *, rtol=1e-11, restart=40, maxiter=400):
+    def adjoint(self, gx, gm, x, mdot, theta, *, rtol=1e-11, restart=200, maxiter=1000):
         """``lambda`` with ``(dR/dz)^T lambda = (gx, gm)`` by right-preconditioned FGMRES."""
         xz = x.detach().requires_grad_(True)
         mz = [m.detach().requires_grad_(True) for m in mdot]
@@ -302,15 +311,23 @@ class SteadyResidual:
             return torch.cat([t.reshape(-1) for t in gs])
 
         def M(v):
+            # block upper triangle of (dR/dz)^T: the mass-flow rows' coupling to x, (dG/dx)^T,
+            # exactly (one reverse pass), the x block by the transposed V-cycle
             parts = split(v)
-            px = self._precondition(parts[0].contiguous())
+            if any(float(p.abs().max()) > 0 for p in parts[1:]):
+                (gx,) = torch.autograd.grad(gmd, [xz], [p.view_as(g) for p, g in
+                                                         zip(parts[1:], gmd)], retain_graph=True)
+                rhs = parts[0] - gx.reshape(-1)
+            else:
+                rhs = parts[0]
+            px = self._precondition(rhs.contiguous())
             return torch.cat([px] + parts[1:])
 
         b = torch.cat([gx.reshape(-1)] + [t.reshape(-1) for t in gm])
         lam, its, res = fgmres(JT, b, M, rtol=rtol, restart=restart, maxiter=maxiter)
         return split(lam), its, res
 
-    def sensitivities(self, rtol=1e-11):
+    def sensitivities(self, rtol=1e-11, restart=200, maxiter=1000):
         """``dJ/dtheta`` ``(n_objectives, n_parameters)``: one adjoint solve per objective (the
         objectives' right-hand sides share the forward hierarchy and residual graph)."""
         x, mdot = self.state()
@@ -326,7 +343,8 @@ class SteadyResidual:
             gx = torch.zeros_like(xz) if gx is None else gx
             gth = torch.zeros_like(th) if gth is None else gth
             gm = [torch.zeros_like(m) if g is None else g for g, m in zip(gm, mz)]
-            lam, its, res = self.adjoint(gx, gm, x, mdot, theta, rtol=rtol)
+            lam, its, res = self.adjoint(gx, gm, x, mdot, theta, rtol=rtol, restart=restart,
+                                         maxiter=maxiter)
             th2 = theta.detach().requires_grad_(True)
             r, gmd, _ = self.residual(x, mdot, th2)
             outs = [r] + gmd
@@ -368,7 +386,8 @@ def fgmres(A, b, M, *, rtol=1e-10, restart=40, maxiter=400):
             for j in range(k + 1):
                 H[j, k] = float(torch.dot(V[j], w))
                 w = w - H[j, k] * V[j]
-            H[k + 1, k] = float(torch.linalg.norm(w))
+            hn = float(torch.linalg.norm(w))
+            H[k + 1, k] = hn
             for j in range(k):
                 t = cs[j] * H[j, k] + sn[j] * H[j + 1, k]
                 H[j + 1, k] = -sn[j] * H[j, k] + cs[j] * H[j + 1, k]
@@ -382,9 +401,9 @@ def fgmres(A, b, M, *, rtol=1e-10, restart=40, maxiter=400):
             it += 1
             k_used = k + 1
             res = abs(g[k + 1]) / bn
-            if res <= rtol or it >= maxiter:
+            if res <= rtol or it >= maxiter or hn == 0.0 or not np.isfinite(res):
                 break
-            V.append(w / H[k + 1, k] if H[k + 1, k] else w)
+            V.append(w / hn)
         y = np.linalg.solve(np.triu(H[:k_used, :k_used]), g[:k_used])
         for j in range(k_used):
             x = x + float(y[j]) * Z[j]
