@@ -13,9 +13,11 @@ is larger than L2, so no flush is needed between steps.
 
 ``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]``
 
-Two further workloads print their own line (``--workload bifurcation``: the ~2M-node
+Three further workloads print their own line (``--workload bifurcation``: the ~2M-node
 transient Y-bifurcation, mixed vs FP64 per BDF2 step; ``--workload ensemble``: 12 vessels
-solved together vs one after another); the default is the headline above.
+solved together vs one after another; ``--workload adjoint``: the adjoint gradient of the
+~500k-node steady Y-bifurcation, checked against central differences); the default is the
+headline above. ``--smoother chebyshev`` runs the headline with the Chebyshev smoother.
 """
 
 from __future__ import annotations
@@ -389,7 +391,8 @@ def ensemble_workload(args):
     seq = solve_sequentially(cases, fl, tol=1e-8, max_iterations=400, linear="b200", log=log)
     torch.cuda.synchronize()
     t = time.perf_counter()
-    ens = B200Ensemble(cases, fl, linear="b200-mixed", linear_options={"autotune": True})
+    ens = B200Ensemble(cases, fl, krylov=args.krylov, linear="b200-mixed",
+                       linear_options={"autotune": True})
     log(f"ensemble set up in {time.perf_counter() - t:.1f} s")
     rep = ens.solve(tol=1e-8, max_iterations=400, log=log)
     torch.cuda.synchronize()
@@ -405,7 +408,8 @@ def ensemble_workload(args):
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
             "dtype": "f64 (FGMRES) / f32 (hierarchy)",
             "config": {"workload": f"{len(cases)} vessels, {sum(sizes):,} nodes in all",
-                       "nodes": sizes, "tol": 1e-8, "mesh_seconds": gen},
+                       "nodes": sizes, "tol": 1e-8, "krylov": args.krylov,
+                       "mesh_seconds": gen},
             "sequential_fp64": {"value": len(cases) / seq["seconds"], "seconds": seq["seconds"],
                                 "outer_iterations": [r["iterations"] for r in seq["instances"]],
                                 "converged": all(r["converged"] for r in seq["instances"])},
@@ -414,6 +418,119 @@ def ensemble_workload(args):
                               "first_converged": [int(x) for x in rep["first_converged"]],
                               "field_error_vs_sequential": err},
             "speedup": seq["seconds"] / t_ens}
+    print(json.dumps(line), flush=True)
+
+
+def adjoint_workload(args):
+    """The adjoint workload: the Y-bifurcation coarsened to about 500k nodes, steady,
+    Carreau-Yasuda blood, a 1 ml/s inlet and RCR outlets (Rp 1e8, C 1e-9, Rd 1e9), a fixed
+    advection blend. Objectives: the two outlet flow fractions and the mean wall shear stress on
+    each daughter's wall beyond the junction; parameters: the inlet flow, each outlet's
+    (Rp, C, Rd) and mu0. Timed: the forward solve to round-off and the adjoint gradient (one
+    FGMRES solve per objective on the transposed Jacobian, preconditioned by the forward
+    hierarchy's transposed V-cycle). Checked: central differences (step 1e-6 relative) of
+    converged solves restarted from the solved state, for every parameter."""
+    import torch
+
+    from zvcfd_b200.fluid import CarreauYasuda, Fluid
+    from zvcfd_b200.lumped import RCR
+    from zvcfd_b200.mesh import y_bifurcation
+    from zvcfd_b200.sensitivity import SteadyResidual
+    from zvcfd_b200.solver import B200Solver
+
+    def log(msg):
+        print(msg, file=sys.stderr, flush=True)
+
+    names = ["Q_in", "Rp1", "C1", "Rd1", "Rp2", "C2", "Rd2", "mu0"]
+    theta0 = np.array([1e-6, 1e8, 1e-9, 1e9, 1e8, 1e-9, 1e9, 0.056])
+    h = 0.25e-3 * (56118.0 / args.adjoint_nodes) ** (1.0 / 3.0)
+    t0 = time.perf_counter()
+    m = y_bifurcation(h, jitter_amount=0.05, seed=0)
+    gen = time.perf_counter() - t0
+    z = {zz.name: k for k, zz in m.zones.items()}
+    f = m.zones[z["wall"]].faces
+    wn = np.unique(f[f >= 0])
+    xw = m.nodes[wn]
+    beyond = xw[:, 2] > 2.5e-3
+    walls = {"daughter1": torch.as_tensor(wn[beyond & (xw[:, 0] > 0)], device="cuda"),
+             "daughter2": torch.as_tensor(wn[beyond & (xw[:, 0] < 0)], device="cuda")}
+
+    def shape(x):
+        return np.clip(1.0 - (x[:, 0] ** 2 + x[:, 1] ** 2) / 2e-3 ** 2, 0.0, None)
+
+    def solve(theta, start=None):
+        q, rp1, c1, rd1, rp2, c2, rd2, mu0 = (float(v) for v in theta)
+        bcs = {z["inlet"]: {"kind": "velocity", "flow_rate": q, "profile": shape},
+               z["outlet1"]: {"kind": "pressure", "lumped": RCR(rp=rp1, c=c1, rd=rd1)},
+               z["outlet2"]: {"kind": "pressure", "lumped": RCR(rp=rp2, c=c2, rd=rd2)},
+               z["wall"]: {"kind": "wall"}}
+        fl = Fluid(1060.0, 0.00345, viscosity=CarreauYasuda(mu_0=mu0))
+        s = B200Solver(m, fl, bcs, advection=1.0, linear_rtol=0.1)
+        if start is not None:
+            s.initialise(U=start[0], P=start[1])
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        rep = s.solve(max_iterations=3000, tol=args.adjoint_tol)
+        torch.cuda.synchronize()
+        return s, rep, time.perf_counter() - t
+
+    s, rep, t_fwd = solve(theta0)
+    log(f"forward: {rep['iterations']} outer iterations, {t_fwd:.1f} s, converged {rep['converged']}")
+    res = SteadyResidual(s, z["inlet"], [z["outlet1"], z["outlet2"]], walls)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    grad, J, info = res.sensitivities(rtol=args.adjoint_rtol, restart=args.adjoint_restart)
+    torch.cuda.synchronize()
+    t_adj = time.perf_counter() - t
+    grad, J = grad.cpu().numpy(), J.cpu().numpy()
+    log(f"adjoint: {t_adj:.1f} s, {info}")
+    start = (s.U.cpu().numpy(), s.P.cpu().numpy())
+    peak_gb = torch.cuda.max_memory_allocated() / 1e9
+    s.close()
+    del res
+    fd = np.zeros_like(grad)
+    fd_solves = []
+    for p in range(len(theta0)):
+        step = 1e-6 * theta0[p]
+        vals = []
+        for sgn in (1.0, -1.0):
+            th = theta0.copy()
+            th[p] += sgn * step
+            sp, rp, tp = solve(th, start)
+            r2 = SteadyResidual(sp, z["inlet"], [z["outlet1"], z["outlet2"]], walls)
+            x2, m2 = r2.state()
+            vals.append(r2.objectives(x2, m2, r2.theta0()).cpu().numpy())
+            fd_solves.append({"iterations": rp["iterations"], "converged": rp["converged"],
+                              "seconds": tp})
+            sp.close()
+            del r2
+        fd[:, p] = (vals[0] - vals[1]) / (2 * step)
+        log(f"fd {names[p]} done")
+    objectives = ["Q1/Q_in", "Q2/Q_in", "WSS daughter1", "WSS daughter2"]
+    err = []
+    for k in range(grad.shape[0]):
+        ref = np.abs(fd[k] * theta0).max()
+        err.append(float(np.abs((grad[k] - fd[k]) * theta0).max() / ref))
+    line = {"metric": "steady adjoint gradient (4 objectives x 8 parameters) vs central differences",
+            "value": 1.0 / t_adj, "unit": "gradients/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"Y-bifurcation, {m.n_nodes:,} nodes, "
+                                   f"{len(m.elements['tet']):,} seeded tets, Carreau-Yasuda, steady",
+                       "lattice_mm": h * 1e3, "forward_tol": args.adjoint_tol,
+                       "adjoint_rtol": args.adjoint_rtol, "restart": args.adjoint_restart,
+                       "fd_step": "1e-6 relative", "mesh_seconds": gen},
+            "forward": {"seconds": t_fwd, "outer_iterations": rep["iterations"],
+                        "converged": rep["converged"]},
+            "adjoint": {"seconds": t_adj, "seconds_per_objective": t_adj / len(objectives),
+                        "adjoint_vs_forward": t_adj / t_fwd,
+                        "krylov": [{"objective": o, **i} for o, i in zip(objectives, info)],
+                        "peak_device_gb": peak_gb},
+            "objectives": dict(zip(objectives, J.tolist())),
+            "gradient": {o: dict(zip(names, g.tolist())) for o, g in zip(objectives, grad)},
+            "central_differences": {o: dict(zip(names, g.tolist())) for o, g in zip(objectives, fd)},
+            "max_error_vs_fd_relative_to_largest_sensitivity": dict(zip(objectives, err)),
+            "capacitance_gradients_zero": bool(np.all(grad[:, [2, 5]] == 0.0)),
+            "fd_solves": fd_solves}
     print(json.dumps(line), flush=True)
 
 
@@ -465,12 +582,19 @@ def gs_pass_bytes(n, nnz, value_bytes=8, vec_bytes=8):
     return (16 * value_bytes + 4) * nnz + 8 * (n + 1) + 16 * value_bytes * n + 3 * 4 * vec_bytes * n
 
 
+def cheb_step_bytes(n, nnz, value_bytes=8, vec_bytes=8):
+    """One Chebyshev step on a level: the level's blocks, indices and row pointers once, each
+    row's 4x4 inverse, b and x_in read, the update read and written, x_out written."""
+    return (16 * value_bytes + 4) * nnz + 8 * (n + 1) + 16 * value_bytes * n + 5 * 4 * vec_bytes * n
+
+
 def vcycle_bytes(stats, value_bytes=8, gs_levels=2, gs_passes=6, jacobi_sweeps=4,
-                 coarse_sweeps=8):
+                 coarse_sweeps=8, smoother="gs", cheb_steps=4):
     """Algorithmic bytes of one V-cycle over the hierarchy ``stats`` (rows and blocks per
     level): Gauss-Seidel passes on the finest ``gs_levels`` (pre 1 + post 2 symmetric sweeps),
     damped Jacobi sweeps below, the residual product, restriction and prolongation of each
-    level, and the permutations in and out of a Gauss-Seidel level's colour order."""
+    level, and the permutations in and out of a Gauss-Seidel level's colour order; with the
+    Chebyshev smoother ``cheb_steps`` steps (pre + post degree) on every level instead."""
     vb = value_bytes
     total = 0
     rows, blocks = stats["levels"], stats["blocks"]
@@ -480,7 +604,9 @@ def vcycle_bytes(stats, value_bytes=8, gs_levels=2, gs_passes=6, jacobi_sweeps=4
         if last and n <= 24:
             total += 16 * n * n * vb + 2 * vec            # dense inverse times the vector
             continue
-        if i < gs_levels:
+        if smoother == "chebyshev":
+            total += (coarse_sweeps if last else cheb_steps) * cheb_step_bytes(n, nnz, vb, vb)
+        elif i < gs_levels:
             total += gs_passes * gs_pass_bytes(n, nnz, vb, vb) + 4 * vec
         else:
             sweeps = coarse_sweeps if last else jacobi_sweeps
@@ -506,10 +632,11 @@ def element_bytes(asm) -> dict:
     return {"assemble": assemble, "assemble_scatter": scatter, "massflow": massflow}
 
 
-def stage_times(solver, peak, value_bytes=8):
+def stage_times(solver, peak, value_bytes=8, smoother="gs"):
     """CUDA-event times and HBM fractions of the outer iteration's stages on the solver's
-    current state, and the Gauss-Seidel pass (the dominant kernel) alone; ``value_bytes`` is
-    the hierarchy's value size (8 FP64, 4 for the FP32 hierarchy)."""
+    current state, and the smoother's pass on the finest level (the dominant kernel) alone:
+    one Gauss-Seidel pass over all colours, or one Chebyshev step; ``value_bytes`` is the
+    hierarchy's value size (8 FP64, 4 for the FP32 hierarchy)."""
     import torch
 
     from zvcfd_b200._lib import call, ptr, stream_ptr
@@ -541,11 +668,19 @@ def stage_times(solver, peak, value_bytes=8):
     st = lin.stats()
     r = b.reshape(-1) - A.matvec(x0)
     t = event_time(lambda: lin.vcycle(r), reps=10)
-    vb = vcycle_bytes(st, value_bytes)
+    vb = vcycle_bytes(st, value_bytes, smoother=smoother,
+                      cheb_steps=lin.presweeps + lin.postsweeps, coarse_sweeps=lin.coarse_sweeps)
     out["vcycle"] = {"ms": t * 1e3, "algorithmic_bytes": vb, "frac": vb / t / 1e9 / peak,
                      "levels": st["levels"], "blocks": st["blocks"]}
     n0, nnz0 = st["levels"][0], st["blocks"][0]
     t = event_time(lambda: call("zvfv_solver_smooth", lin._h, 0, 1, stream_ptr()), reps=10)
+    if smoother == "chebyshev":
+        cb = cheb_step_bytes(n0, nnz0, value_bytes, value_bytes)
+        kern = "double, double>" if value_bytes == 8 else "float, float>"
+        out["gs_pass"] = {"ms": t * 1e3, "algorithmic_bytes": cb, "frac": cb / t / 1e9 / peak,
+                          "kernel": f"k_cheby<{_lanes(n0, nnz0)}, false, false, " + kern,
+                          "launches": 1, "what": "one Chebyshev step on the finest level"}
+        return out, st
     gb = gs_pass_bytes(n0, nnz0, value_bytes, value_bytes)
     kern = "double, double>" if value_bytes == 8 else "float, float>"
     out["gs_pass"] = {"ms": t * 1e3, "algorithmic_bytes": gb, "frac": gb / t / 1e9 / peak,
@@ -553,6 +688,12 @@ def stage_times(solver, peak, value_bytes=8):
                                 + kern,
                       "launches": int(_gs_colours(lin))}
     return out, st
+
+
+def _lanes(n, nnz):
+    """Lanes per row of the hierarchy's row kernels (without the autotuner)."""
+    per = nnz / max(n, 1)
+    return 32 if per > 40 else (16 if per > 12 else 8)
 
 
 def _gs_colours(lin):
@@ -564,7 +705,7 @@ def _gs_colours(lin):
     return lib.zvfv_launch_count() - before
 
 
-def iteration_bytes(solver, stats, linear_iterations, value_bytes=8):
+def iteration_bytes(solver, stats, linear_iterations, value_bytes=8, smoother="gs"):
     """Algorithmic bytes of one outer iteration (mean over the timed window): the element
     stage, two gradient passes, the boundary pass (matrix read and written once), per Krylov
     step one V-cycle, one operator product and the Arnoldi passes (CGS2 over the basis, mean
@@ -573,7 +714,10 @@ def iteration_bytes(solver, stats, linear_iterations, value_bytes=8):
     eb = element_bytes(solver.asm)
     its = float(np.mean(linear_iterations)) if linear_iterations else 0.0
     n4 = 4 * N * 8
-    krylov = vcycle_bytes(stats, value_bytes) + spmv_bytes(N, nnzb) + (4 * (its / 2 + 1) + 8) * n4
+    lin = solver.linear
+    vc = vcycle_bytes(stats, value_bytes, smoother=smoother,
+                      cheb_steps=lin.presweeps + lin.postsweeps, coarse_sweeps=lin.coarse_sweeps)
+    krylov = vc + spmv_bytes(N, nnzb) + (4 * (its / 2 + 1) + 8) * n4
     grad = 2 * (nnzb * (24 + 4) + 8 * N + 4 * 8 * N + 12 * 8 * N)
     finalise = 2 * 128 * nnzb + 8 * nnzb + 4 * n4
     refresh = sum(2 * 16 * 8 * nb for nb in stats["blocks"])
@@ -592,15 +736,27 @@ def main():
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stages", action="store_true")
-    ap.add_argument("--workload", default="tube", choices=["tube", "bifurcation", "ensemble"],
-                    help="tube: the headline (default); bifurcation: config-2 transient; "
-                         "ensemble: config-4 batch")
+    ap.add_argument("--workload", default="tube",
+                    choices=["tube", "bifurcation", "ensemble", "adjoint"],
+                    help="tube: the headline (default); bifurcation: the 2M-node transient; "
+                         "ensemble: the 12-vessel batch; adjoint: the 500k-node steady gradient")
     ap.add_argument("--nodes", type=int, default=2_000_000, help="bifurcation workload size")
     ap.add_argument("--loops", type=int, default=5,
                     help="bifurcation: coefficient loops per time step at most (the reference's 5)")
     ap.add_argument("--instances", type=int, default=12, help="ensemble workload size")
     ap.add_argument("--max-nodes", type=int, default=1_200_000,
                     help="largest ensemble instance")
+    ap.add_argument("--krylov", default="segmented", choices=["segmented", "union"],
+                    help="ensemble: one Krylov recurrence per instance, or one over the union")
+    ap.add_argument("--adjoint-nodes", type=int, default=500_000, help="adjoint workload size")
+    ap.add_argument("--adjoint-tol", type=float, default=1e-11,
+                    help="adjoint workload: the forward solves' residual target")
+    ap.add_argument("--adjoint-rtol", type=float, default=1e-10,
+                    help="adjoint workload: the adjoint FGMRES tolerance")
+    ap.add_argument("--adjoint-restart", type=int, default=60,
+                    help="adjoint workload: the adjoint FGMRES restart length")
+    ap.add_argument("--smoother", default="gs", choices=["gs", "chebyshev", "jacobi"],
+                    help="tube: the AMG smoother of both solvers")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark the timed steps with an NVTX range 'timed' (for ncu --nvtx-include)")
     args = ap.parse_args()
@@ -615,7 +771,8 @@ def main():
 
         torch.cuda.set_device(local)
         if rank == 0:
-            (bifurcation_workload if args.workload == "bifurcation" else ensemble_workload)(args)
+            {"bifurcation": bifurcation_workload, "ensemble": ensemble_workload,
+             "adjoint": adjoint_workload}[args.workload](args)
         return
 
     import torch
@@ -634,8 +791,9 @@ def main():
     m, fl, bcs = make_case(args.axial)
     # two identical solvers: `value` is timed on one, `e2e` on the other over the same outer
     # iterations (warm-up + 1 .. warm-up + steps) - the device work is deterministic
-    solver = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1)
-    twin = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1)
+    lopts = {"smoother": args.smoother}
+    solver = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1, linear_options=lopts)
+    twin = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1, linear_options=lopts)
     for _ in range(args.warmup):
         solver.iterate()
         twin.iterate()
@@ -683,7 +841,7 @@ def main():
     same = [r["linear_iterations"] for r in recs] == [r["linear_iterations"] for r in twin_recs]
     twin.close()
     # mixed precision on the same case and window
-    mixed = B200Solver(m, fl, bcs, linear="b200-mixed", linear_rtol=0.1)
+    mixed = B200Solver(m, fl, bcs, linear="b200-mixed", linear_rtol=0.1, linear_options=lopts)
     for _ in range(args.warmup):
         mixed.iterate()
     melapsed, mrecs = run_steps(mixed, args.steps)
@@ -703,9 +861,10 @@ def main():
                      "fp64_frac": sp["fp64"]["gbs"] / peak, "nnzb": nnzb, "rows": n}
     roof = None
     if not args.no_stages:
-        stages, hstats = stage_times(solver, peak)
-        mstages, _ = stage_times(mixed, peak, 4)
-        ib = iteration_bytes(solver, hstats, extra["fp64_linear_iterations"])
+        stages, hstats = stage_times(solver, peak, smoother=args.smoother)
+        mstages, _ = stage_times(mixed, peak, 4, smoother=args.smoother)
+        ib = iteration_bytes(solver, hstats, extra["fp64_linear_iterations"],
+                             smoother=args.smoother)
         extra["stages"] = {"fp64": stages,
                            "mixed": {k: mstages[k] for k in ("vcycle", "gs_pass")}}
         extra["outer_iteration_roofline"] = {
@@ -714,17 +873,18 @@ def main():
             "note": "sum of the algorithmic bytes of every stage of one outer iteration "
                     "(mean Krylov steps of the window) over ms_per_step"}
         g = stages["gs_pass"]
-        roof = {"kernel": g["kernel"] + " (one pass over all colours of the finest level)",
+        what = g.get("what", "one pass over all colours of the finest level")
+        roof = {"kernel": f"{g['kernel']} ({what})",
                 "bound": "hbm", "achieved": g["algorithmic_bytes"] / (g["ms"] * 1e-3) / 1e9,
                 "peak": peak, "unit": "GB/s", "frac": g["frac"], "peak_source": peak_source,
                 "algorithmic_bytes": g["algorithmic_bytes"],
-                "traffic": None if GS_TRAFFIC_PER_ALGORITHMIC_BYTE is None
-                else GS_TRAFFIC_PER_ALGORITHMIC_BYTE * g["algorithmic_bytes"],
-                "traffic_source": GS_TRAFFIC_SOURCE}
+                "traffic": None if GS_TRAFFIC_PER_ALGORITHMIC_BYTE is None or
+                args.smoother != "gs" else GS_TRAFFIC_PER_ALGORITHMIC_BYTE * g["algorithmic_bytes"],
+                "traffic_source": GS_TRAFFIC_SOURCE if args.smoother == "gs" else None}
     if not args.no_converge and rank == 0:
         conv = {}
         for tag, lin in (("fp64", "b200"), ("mixed", "b200-mixed")):
-            s = B200Solver(m, fl, bcs, linear=lin, linear_rtol=0.1)
+            s = B200Solver(m, fl, bcs, linear=lin, linear_rtol=0.1, linear_options=lopts)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             rep = s.solve(max_iterations=400, tol=1e-8)
@@ -762,6 +922,7 @@ def main():
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "nodes": N, "blocks": nnzb,
                            "precision": "fp64 (mixed below)", "linear_rtol": 0.1,
+                           "smoother": args.smoother,
                            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32 * N,
                         "d2h_bytes_per_step": 32 * N + 8 * 29},

@@ -225,8 +225,12 @@ int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const i
  * API the reference binds (AMGX_config_create / resources / matrix / solver handles,
  * zvcfd/fv/linear.py:728-739, :846-868, :905-955) and its own ACM (linear.py:328-518).
  * create: precision 0 FP64, 1 FP32 hierarchy; smoother 0 damped block Jacobi, 1 symmetric
- * multicolour block Gauss-Seidel (AmgX's MULTICOLOR_GS of the `gs` preset, linear.py:571-598);
- * strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
+ * multicolour block Gauss-Seidel (AmgX's MULTICOLOR_GS of the `gs` preset, linear.py:571-598),
+ * 2 block-Jacobi-preconditioned Chebyshev polynomials of degree presweeps / postsweeps
+ * (coarse_sweeps on a coarsest level too large for the dense inverse) on every level, over
+ * [hi / cheb_ratio, hi], hi = 1.1 x the largest eigenvalue of D^-1 A estimated by power
+ * iteration at each rebuild (AmgX's CHEBYSHEV smoother, which the reference's presets do not
+ * select; no colouring, every step one pass over the level); strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
  * directions of each coupling (the default of the Python back end: convection otherwise
  * stalls the pairwise matching). rebuild_every > 0 re-aggregates every that many
  * set-ups (the reference's ACM, linear.py:337-348); 0 keeps the aggregates until a solve fails
@@ -262,9 +266,10 @@ int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
  * sweeps, the dense coarsest inverse transposed on every level): the preconditioner of the
  * parameter adjoint's FGMRES; no reference counterpart (the reference has no adjoint) */
 int zvfv_solver_vcycle_t(void *handle, const double *r, double *z, void *stream);
-/* `passes` forward multicolour Gauss-Seidel passes on level `level` (a Gauss-Seidel level)
- * over that level's own work vectors: the smoother kernel alone, for timing (no reference
- * counterpart: AmgX's smoother is internal to its V-cycle). */
+/* `passes` forward multicolour Gauss-Seidel passes on level `level` (a Gauss-Seidel level),
+ * or with the Chebyshev smoother `passes` Chebyshev steps on any level but a dense coarsest
+ * one, over that level's own work vectors (overwritten): the smoother kernel alone, for timing
+ * (no reference counterpart: AmgX's smoother is internal to its V-cycle). */
 int zvfv_solver_smooth(void *handle, int level, int passes, void *stream);
 /* Hierarchy options beyond create (each takes effect at the next set-up, which rebuilds):
  *   "autotune" (0/1, default 0): after each rebuild, every level of 2048 rows or more times one
@@ -273,10 +278,13 @@ int zvfv_solver_smooth(void *handle, int level, int passes, void *stream);
  *   "gs_levels" (default 2): the finest levels smoothed by Gauss-Seidel, Jacobi below;
  *   "jacobi_sweeps" (default 2), "jacobi_omega" (default 0.7): the block-Jacobi smoothing of
  *       the levels below (the reference ACM's damped Jacobi, zvcfd/fv/linear.py:343, :480-502);
- *   "rebuild_ratio" (default 1.5): the adaptive rebuild threshold.
+ *   "rebuild_ratio" (default 1.5): the adaptive rebuild threshold;
+ *   "cheb_ratio" (> 1, default 10), "cheb_power" (>= 2, default 10): the Chebyshev interval's
+ *       ratio and the power-iteration steps of its bound.
  * Unknown names or out-of-range values return ZVFV_BAD_ARGUMENT. */
 int zvfv_solver_set_option(void *handle, const char *name, double value);
-/* The value of an option above, or a counter: "rebuilds" (hierarchy builds so far), "setups". */
+/* The value of an option above, or a counter: "rebuilds" (hierarchy builds so far), "setups",
+ * or "cheb_lmax" (the finest level's largest-eigenvalue estimate of the Chebyshev smoother). */
 int zvfv_solver_get_option(void *handle, const char *name, double *value);
 /* hierarchy sizes (ACM.stats, zvcfd/fv/linear.py:515-518) */
 int zvfv_solver_stats(void *handle, int max_levels, int *levels, int64_t *rows, int64_t *blocks);

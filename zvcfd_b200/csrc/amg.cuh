@@ -13,7 +13,9 @@
 //    entry in the same form (AmgX's `aggregation_edge_weight_component: 3`, linear.py:95-102);
 //  * coarse operators: Galerkin with piecewise-constant transfer, the sum of the blocks of
 //    each aggregate pair (linear.py:437-454), in a fixed order (deterministic);
-//  * smoothing: damped block Jacobi with the inverse of each 4x4 diagonal block;
+//  * smoothing: damped block Jacobi with the inverse of each 4x4 diagonal block, symmetric
+//    multicolour block Gauss-Seidel on the finest levels, or block-Jacobi-preconditioned
+//    Chebyshev polynomials (the largest eigenvalue of D^-1 A by power iteration at set-up);
 //  * coarsest level: the explicit inverse of the dense matrix (Gauss-Jordan with partial
 //    pivoting in one CTA), or smoothing sweeps when coarsening stalls above that size.
 //
@@ -478,6 +480,116 @@ k_jacobi_t(long long n, const long long *__restrict__ tptr, const int *__restric
     }
 }
 
+// ------------------------------------------------------------------ Chebyshev smoothing
+
+// One step of block-Jacobi-preconditioned Chebyshev iteration (Saad, Iterative Methods for
+// Sparse Linear Systems, 2nd ed., Algorithm 12.1, on D^-1 A; Adams, Brezina, Hu and
+// Tuminaro, J. Comput. Phys. 188 (2003), for its use as a multigrid smoother):
+//   z = D^-1 (b - A x_in),  d <- cd d + cz z,  x_out = x_in + d.
+// The row's update d is kept in place (each row reads and writes only its own four entries);
+// FIRST: x_in = 0 and no previous update (x_out = d = cz D^-1 b); cd == 0 starts a sequence
+// from a nonzero x_in without reading d. Rows split over G lanes as in the Jacobi sweep.
+// TR: the same step on A^T (through the transpose structure) and D^-T.
+template <int G, bool FIRST, bool TR, typename V, typename T>
+__global__ void __launch_bounds__(256)
+k_cheby(long long n, const long long *__restrict__ ptr_, const int *__restrict__ idx,
+        const long long *__restrict__ tperm, const V *__restrict__ data,
+        const V *__restrict__ dinv, const T *__restrict__ b, const T *__restrict__ xin,
+        T *__restrict__ xout, T *__restrict__ d, T cd, T cz) {
+    constexpr int S = G / 4;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = gid / G;
+    const int lane = threadIdx.x % G;
+    const int slot = lane / 4, r = lane % 4;
+    T acc = 0;
+    if (!FIRST && row < n) {
+        const long long p1 = ptr_[row + 1];
+        for (long long p = ptr_[row] + slot; p < p1; p += S) {
+            const int j = idx[p];
+            const Vec4<T> xv = Vec4<T>::load(xin + (long long)j * 4);
+            if (TR) {
+                const V *blk = data + tperm[p] * 16;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc += (T)__ldg(blk + c * 4 + r) * xv.v[c];
+            } else {
+                const Vec4<V> a = Vec4<V>::load_stream(data + p * 16 + r * 4);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc += (T)a.v[c] * xv.v[c];
+            }
+        }
+#pragma unroll
+        for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    }
+    T res = 0;
+    if (row < n) res = b[row * 4 + r] - acc;
+    const int base = (threadIdx.x % 32) / G * G;
+    T rc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rc[c] = __shfl_sync(0xffffffffu, res, base + c);
+    if (row < n && slot == 0) {
+        T z = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) z += (T)dinv[row * 16 + (TR ? c * 4 + r : r * 4 + c)] * rc[c];
+        const long long i = row * 4 + r;
+        T step = cz * z;
+        if (!FIRST && cd != (T)0) step += cd * d[i];
+        d[i] = step;
+        xout[i] = (FIRST ? (T)0 : xin[i]) + step;
+    }
+}
+
+// Per-CTA partial sums of squares of v[0..m) (a fixed grid: the fold is deterministic).
+template <typename T>
+__global__ void __launch_bounds__(256) k_sumsq(long long m, const T *__restrict__ v,
+                                               double *__restrict__ partial) {
+    __shared__ double red[8];
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double e = (double)v[i];
+        s += e * e;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += red[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// out = in / sqrt(sum of the nparts partials) (every CTA folds the partials in one order).
+template <typename T>
+__global__ void __launch_bounds__(256) k_scale_by(long long m, int nparts,
+                                                  const double *__restrict__ partial,
+                                                  const T *__restrict__ in, T *__restrict__ out) {
+    __shared__ double inv;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < nparts; ++k) t += partial[k];
+        inv = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
+    }
+    __syncthreads();
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = (T)((double)in[i] * inv);
+}
+
+// A deterministic start vector for the power iteration: values in [0.5, 1.5) from a hash of
+// the index (positive, so that it is not orthogonal to the dominant eigenvector of D^-1 A).
+template <typename T>
+__global__ void k_fill_start(long long m, T *__restrict__ v) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    unsigned long long h = (unsigned long long)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 27;
+    v[i] = (T)(0.5 + (double)(h >> 11) * (1.0 / 9007199254740992.0));
+}
+
 // ------------------------------------------------------------------ multicolour Gauss-Seidel
 
 // In-place block Gauss-Seidel over the rows of one colour (rows[0..count)): rows of a colour
@@ -771,6 +883,8 @@ struct Level {
     double *pdata64 = nullptr, *pdinv64 = nullptr;
     float *pdata32 = nullptr, *pdinv32 = nullptr;
     void *pb = nullptr;                          // the level's right-hand side, colour-ordered
+    // Chebyshev smoothing: the estimated largest eigenvalue of D^-1 A (power iteration)
+    double cheb_lmax = 0.0;
     // dense coarsest
     bool dense = false;
     double *inv64 = nullptr;
@@ -781,7 +895,8 @@ struct Level {
 
 struct Params {
     int precision = 0;       // 0 FP64 cycle, 1 FP32 cycle
-    int smoother = 1;        // 0 damped block Jacobi, 1 symmetric multicolour block Gauss-Seidel
+    int smoother = 1;        // 0 damped block Jacobi, 1 symmetric multicolour block Gauss-Seidel,
+                             // 2 block-Jacobi-preconditioned Chebyshev (sweeps = degree)
     int gs_levels = 2;       // with Gauss-Seidel: the finest levels that use it (Jacobi below)
     int jacobi_sweeps = 2;   // damped block-Jacobi sweeps (pre and post) below them
     double jacobi_omega = 0.7;
@@ -794,6 +909,8 @@ struct Params {
     int rebuild_every = 0;   // > 0: re-aggregate every this many set-ups; 0: adaptively
     double rebuild_ratio = 1.5;   // adaptive: rebuild after a solve needing more iterations
     int autotune = 0;        // 1: time each level's smoother at 8, 16 and 32 lanes per row
+    double cheb_ratio = 10.0;   // Chebyshev: the interval [hi / ratio, hi], hi = 1.1 lambda_max
+    int cheb_power = 10;        // power-iteration steps estimating lambda_max of D^-1 A
 };
 
 inline int lanes_for(long long n, long long nnz) {

@@ -277,6 +277,11 @@ class Hierarchy {
         }
         ZV_TRY(compute_values());
         if (rebuild && prm.autotune) ZV_TRY(prm.precision == 1 ? autotune<float>() : autotune<double>());
+        // Chebyshev: the spectral bound of every level, with the aggregates (a rebuild); the
+        // values re-summed between rebuilds move it little, and a solve that degrades triggers
+        // the adaptive rebuild
+        if (rebuild && prm.smoother == 2)
+            ZV_TRY(prm.precision == 1 ? estimate_spectra<float>() : estimate_spectra<double>());
         return OK;
     }
 
@@ -787,6 +792,8 @@ class Hierarchy {
     int cycle(size_t l);
     template <typename T>
     int autotune();
+    template <typename T>
+    int estimate_spectra();
 };
 
 __global__ void k_iota_i32(int *p, long long n) {
@@ -848,6 +855,30 @@ void jacobi_t(int lanes, long long n, const Level &v, const V *data, const V *di
             k_jacobi_t<32, FIRST, V, T><<<grid_for(n * 32, 256), 256, 0, st>>>(n, v.tptr, v.trow, v.tperm, data,
                                                                              dinv, b, xin, xout, omega); count_launch();
     }
+}
+
+// one Chebyshev step on level v (k_cheby): A through the level's CSR, or with TR A^T through
+// its transpose structure
+template <bool FIRST, bool TR, typename V, typename T>
+void cheby(const Level &v, const V *data, const V *dinv, const T *b, const T *xin, T *xout, T *d,
+           T cd, T cz, cudaStream_t st) {
+    const long long *p = TR ? v.tptr : v.indptr;
+    const int *ix = TR ? v.trow : v.indices;
+    const long long n = v.n;
+    switch (v.lanes) {
+        case 8:
+            k_cheby<8, FIRST, TR, V, T><<<grid_for(n * 8, 256), 256, 0, st>>>(n, p, ix, v.tperm, data, dinv, b,
+                                                                            xin, xout, d, cd, cz);
+            break;
+        case 16:
+            k_cheby<16, FIRST, TR, V, T><<<grid_for(n * 16, 256), 256, 0, st>>>(n, p, ix, v.tperm, data, dinv, b,
+                                                                              xin, xout, d, cd, cz);
+            break;
+        default:
+            k_cheby<32, FIRST, TR, V, T><<<grid_for(n * 32, 256), 256, 0, st>>>(n, p, ix, v.tperm, data, dinv, b,
+                                                                              xin, xout, d, cd, cz);
+    }
+    count_launch();
 }
 
 // A launch of 256-thread CTAs that may begin while the previous kernel in the stream is still
@@ -986,6 +1017,54 @@ int Hierarchy::cycle(size_t l) {
         sgs(prm.postsweeps);
         return launch_status("v-cycle");
     }
+    if (prm.smoother == 2) {
+        // Chebyshev polynomials of degree pre and post in D^-1 A on [hi / ratio, hi],
+        // hi = 1.1 lambda_max: centre theta, half-width delta, and the three-term recurrence
+        // rho_k = 1 / (2 sigma - rho_{k-1}), sigma = theta / delta, rho_0 = 1 / sigma
+        const double hi = 1.1 * v.cheb_lmax, lo = hi / prm.cheb_ratio;
+        const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+        T *d = static_cast<T *>(v.r);          // the update: r is free while smoothing
+        auto steps = [&](int degree, bool from_zero) {
+            double rho = 1.0 / sigma;
+            for (int k = 0; k < degree; ++k) {
+                double cd = 0.0, cz = 1.0 / theta;
+                if (k > 0) {
+                    const double next = 1.0 / (2.0 * sigma - rho);
+                    cd = next * rho;
+                    cz = 2.0 * next / delta;
+                    rho = next;
+                }
+                if (k == 0 && from_zero) {
+                    cheby<true, TRANS, V, T>(v, data, dinv, b, nullptr, static_cast<T *>(v.x), d, (T)cd,
+                                             (T)cz, st);
+                    continue;
+                }
+                cheby<false, TRANS, V, T>(v, data, dinv, b, static_cast<const T *>(v.x),
+                                          static_cast<T *>(v.x2), d, (T)cd, (T)cz, st);
+                std::swap(v.x, v.x2);
+            }
+        };
+        if (pre > 0) {
+            steps(pre, true);
+        } else {
+            cudaMemsetAsync(v.x, 0, v.n * 4 * sizeof(T), st);
+        }
+        if (last) return launch_status("coarse smoothing");
+        T *r = static_cast<T *>(v.r);
+        if (TRANS)
+            ZV_TRY(bsr_spmv_t_launch<true, V, T>(v.lanes, v.n, v.tptr, v.trow, v.tperm, data,
+                                                 static_cast<const T *>(v.x), b, r, st));
+        else
+            ZV_TRY(bsr_spmv_launch<true, V, T>(v.lanes, v.n, v.indptr, v.indices, data,
+                                               static_cast<const T *>(v.x), b, r, st));
+        Level &c = L[l + 1];
+        k_restrict<T><<<grid_for(c.n * 4, 256), 256, 0, st>>>(c.n, v.mptr, v.mem, r, static_cast<T *>(c.b)); count_launch();
+        ZV_TRY((cycle<T, TRANS>(l + 1)));
+        k_prolong_add<T><<<grid_for(v.n * 4, 256), 256, 0, st>>>(v.n, v.agg, static_cast<const T *>(c.x),
+                                                                static_cast<T *>(v.x)); count_launch();
+        steps(prm.postsweeps, false);
+        return launch_status("v-cycle");
+    }
     auto sweep = [&](bool first, const T *xin, T *xout) {
         if (TRANS) {
             if (first) jacobi_t<true>(v.lanes, v.n, v, data, dinv, b, xin, xout, omega, st);
@@ -1070,6 +1149,44 @@ int Hierarchy::autotune() {
     cudaEventDestroy(e1);
     if (rc == OK) rc = launch_status("autotune");
     return rc;
+}
+
+// The largest eigenvalue of D^-1 A on every smoothed level, by cheb_power steps of the power
+// iteration from a fixed positive start: x <- w / |w|, w = D^-1 A x (the bound of the
+// Chebyshev interval; A^T shares it, D^-T A^T being similar to the transpose of D^-1 A).
+// Runs in the cycle's precision on the level's work vectors; the last |w| (of a unit x) is the
+// estimate, folded on the host in a fixed order.
+template <typename T>
+int Hierarchy::estimate_spectra() {
+    using V = T;
+    const int np = std::max(1, 2 * sm_count());
+    double *partial;
+    ZV_TRY(scratch.get(&partial, np));
+    std::vector<double> host(np);
+    for (Level &v : L) {
+        if (v.dense) continue;
+        const long long m = v.n * 4;
+        const V *data = CyclePick<T>::data(v), *dinv = CyclePick<T>::dinv(v);
+        T *x = static_cast<T *>(v.x), *y = static_cast<T *>(v.r), *w = static_cast<T *>(v.x2);
+        const unsigned g = (unsigned)std::min<long long>(grid_for(m, 256), np);
+        k_fill_start<T><<<grid_for(m, 256), 256, 0, st>>>(m, x); count_launch();
+        for (int k = 0; k < std::max(prm.cheb_power, 2); ++k) {
+            ZV_TRY((bsr_spmv_launch<false, V, T>(v.lanes, v.n, v.indptr, v.indices, data, x, nullptr, y, st)));
+            jacobi<true, V, T>(v.lanes, v.n, v.indptr, v.indices, data, dinv, y, nullptr, w, (T)1, st);
+            cudaMemsetAsync(partial, 0, np * sizeof(double), st);
+            k_sumsq<T><<<g, 256, 0, st>>>(m, w, partial); count_launch();
+            k_scale_by<T><<<g, 256, 0, st>>>(m, np, partial, w, x); count_launch();
+        }
+        ZV_TRY(cuda_status(cudaMemcpyAsync(host.data(), partial, np * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st), "spectral estimate"));
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "spectral estimate"));
+        double sum = 0.0;
+        for (double p : host) sum += p;
+        const double lmax = std::sqrt(sum);
+        v.cheb_lmax = std::isfinite(lmax) && lmax > 0.0 ? lmax : 2.0;
+    }
+    scratch.release();
+    return launch_status("spectral estimate");
 }
 
 // ------------------------------------------------------------------ the solver handle
@@ -1279,7 +1396,7 @@ extern "C" {
 int zvfv_solver_create(void **handle, int precision, int smoother, int strength, int passes,
                        int presweeps, int postsweeps, double omega, int coarse_sweeps,
                        int max_levels, int rebuild_every, int restart) {
-    if (!handle || precision < 0 || precision > 1 || smoother < 0 || smoother > 1 || restart < 1 ||
+    if (!handle || precision < 0 || precision > 1 || smoother < 0 || smoother > 2 || restart < 1 ||
         restart > MAXV - 1 || passes < 1 || presweeps < 1 || postsweeps < 0 || max_levels < 1) {
         set_error("solver_create: bad arguments");
         return BAD_ARGUMENT;
@@ -1384,8 +1501,10 @@ int zvfv_solver_vcycle_t(void *handle, const double *r, double *z, void *stream)
 }
 
 // `passes` forward Gauss-Seidel passes over the colours of level `level` (one of the
-// Gauss-Seidel levels) on the level's own work vectors, in the hierarchy's precision: the
-// smoother kernel alone, for timing it (the V-cycle graph runs the same launches).
+// Gauss-Seidel levels), or with the Chebyshev smoother `passes` Chebyshev steps on any level
+// but a dense coarsest one, on the level's own work vectors, in the hierarchy's precision: the
+// smoother kernel alone, for timing it (the V-cycle graph runs the same launches). The work
+// vectors' contents are overwritten; the V-cycle does not depend on them between cycles.
 int zvfv_solver_smooth(void *handle, int level, int passes, void *stream) {
     Solver *s = static_cast<Solver *>(handle);
     if (!s || !s->data || level < 0 || level >= (int)s->H.L.size() || passes < 1) {
@@ -1393,11 +1512,32 @@ int zvfv_solver_smooth(void *handle, int level, int passes, void *stream) {
         return BAD_ARGUMENT;
     }
     Level &v = s->H.L[level];
+    const cudaStream_t st = as_stream(stream);
+    if (s->H.prm.smoother == 2 && !v.dense) {
+        // alternate x and x2 without swapping the level's pointers (the captured V-cycle
+        // graph keeps them); after the first step, the recurrence's limiting coefficients
+        const double hi = 1.1 * v.cheb_lmax, lo = hi / s->H.prm.cheb_ratio;
+        const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+        const double rho = sigma - std::sqrt(sigma * sigma - 1.0);
+        for (int q = 0; q < passes; ++q) {
+            void *xin = (q % 2) ? v.x2 : v.x, *xout = (q % 2) ? v.x : v.x2;
+            const double c = q == 0 ? 0.0 : rho * rho, cz = q == 0 ? 1.0 / theta : 2.0 * rho / delta;
+            if (s->H.prm.precision == 1)
+                cheby<false, false, float, float>(v, v.data32, v.dinv32, static_cast<const float *>(v.b),
+                                                  static_cast<const float *>(xin), static_cast<float *>(xout),
+                                                  static_cast<float *>(v.r), (float)c, (float)cz, st);
+            else
+                cheby<false, false, double, double>(v, v.data, v.dinv64, static_cast<const double *>(v.b),
+                                                    static_cast<const double *>(xin),
+                                                    static_cast<double *>(xout),
+                                                    static_cast<double *>(v.r), c, cz, st);
+        }
+        return launch_status("solver_smooth");
+    }
     if (v.gs_off.empty() || !v.pb || !v.x2) {
-        set_error("solver_smooth: level %d is not smoothed by Gauss-Seidel", level);
+        set_error("solver_smooth: level %d is not smoothed by Gauss-Seidel or Chebyshev", level);
         return BAD_ARGUMENT;
     }
-    const cudaStream_t st = as_stream(stream);
     for (int q = 0; q < passes; ++q) {
         if (s->H.prm.precision == 1)
             gs_pass<false, float, float>(v, v.pdata32, v.pdinv32, static_cast<const float *>(v.pb),
@@ -1424,6 +1564,8 @@ int zvfv_solver_set_option(void *handle, const char *name, double value) {
     else if (opt == "jacobi_sweeps" && value >= 1) p.jacobi_sweeps = (int)value;
     else if (opt == "jacobi_omega" && value > 0) p.jacobi_omega = value;
     else if (opt == "rebuild_ratio" && value >= 1) p.rebuild_ratio = value;
+    else if (opt == "cheb_ratio" && value > 1) p.cheb_ratio = value;
+    else if (opt == "cheb_power" && value >= 2) p.cheb_power = (int)value;
     else {
         set_error("solver_set_option: unknown option or bad value: %s = %g", name, value);
         return BAD_ARGUMENT;
@@ -1445,6 +1587,9 @@ int zvfv_solver_get_option(void *handle, const char *name, double *value) {
     else if (opt == "jacobi_sweeps") *value = p.jacobi_sweeps;
     else if (opt == "jacobi_omega") *value = p.jacobi_omega;
     else if (opt == "rebuild_ratio") *value = p.rebuild_ratio;
+    else if (opt == "cheb_ratio") *value = p.cheb_ratio;
+    else if (opt == "cheb_power") *value = p.cheb_power;
+    else if (opt == "cheb_lmax") *value = s->H.L.empty() ? 0.0 : s->H.L[0].cheb_lmax;
     else if (opt == "rebuilds") *value = (double)s->H.rebuilds;
     else if (opt == "setups") *value = (double)s->H.setups;
     else {
