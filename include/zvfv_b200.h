@@ -230,7 +230,11 @@ int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const i
  * (coarse_sweeps on a coarsest level too large for the dense inverse) on every level, over
  * [hi / cheb_ratio, hi], hi = 1.1 x the largest eigenvalue of D^-1 A estimated by power
  * iteration at each rebuild (AmgX's CHEBYSHEV smoother, which the reference's presets do not
- * select; no colouring, every step one pass over the level); strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
+ * select; no colouring, every step one pass over the level), 3 multicolour DILU on the
+ * Gauss-Seidel levels (AmgX's MULTICOLOR_DILU of the `dilu` presets, linear.py:571-608: the
+ * diagonal E_i = A_ii - sum over earlier colours A_ij E_j^-1 A_ji, one step
+ * x += omega M^-1 (b - A x) with M = (E + L) E^-1 (E + U); the transposed cycle smooths those
+ * levels by transposed Gauss-Seidel); strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
  * directions of each coupling (the default of the Python back end: convection otherwise
  * stalls the pairwise matching). rebuild_every > 0 re-aggregates every that many
  * set-ups (the reference's ACM, linear.py:337-348); 0 keeps the aggregates until a solve fails
@@ -260,6 +264,21 @@ int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, i
                         const int64_t *u_len, const int64_t *const *w_idx,
                         const double *const *w_val, const int64_t *w_len, int *iterations,
                         double *residual, int *converged, void *stream);
+/* FGMRES with one Krylov recurrence per segment of rows: the block-diagonal system of
+ * independent instances (an ensemble's union). row_bounds: n_segments + 1 ascending host values
+ * from 0 to n. The operator and the V-cycle act on all segments at once; inner products, norms,
+ * Hessenberg columns, rotations and step lengths are per segment, and each segment stops at
+ * rtol times its own initial residual (floor 1e-13 of its right-hand side's norm). The solve
+ * ends when all have, or after maxiter Krylov steps (shared). residuals, converged: n_segments
+ * host values. No reference counterpart (the reference solves one problem per solver).
+ * Other arguments as zvfv_solver_solve. */
+int zvfv_solver_solve_segmented(void *handle, int n_segments, const int64_t *row_bounds,
+                                const double *b, double *x, double rtol, int maxiter,
+                                int n_lowrank, const int64_t *const *u_idx,
+                                const double *const *u_val, const int64_t *u_len,
+                                const int64_t *const *w_idx, const double *const *w_val,
+                                const int64_t *w_len, int *iterations, double *residuals,
+                                int *converged, void *stream);
 /* z = one V-cycle applied to r (AMGX.vcycle, zvcfd/fv/linear.py:905-918) */
 int zvfv_solver_vcycle(void *handle, const double *r, double *z, void *stream);
 /* z = one V-cycle of the transposed hierarchy applied to r (A^T, D^-T, transposed Gauss-Seidel

@@ -2,7 +2,8 @@
 
 Three small vessels of different kinds and sizes (a straight tet pipe, a curved hex/prism
 tube, a tet Y-bifurcation), each with its own inlet flow and RCR outlets, solved together as
-one block-diagonal system with the FP32 hierarchy and the lanes autotuner, reach each
+one block-diagonal system with the FP32 hierarchy and the lanes autotuner (one Krylov
+recurrence per instance, or one over the union), reach each
 instance's own FP64 solution (solved alone; both to relative changes below 1e-9) to 1e-7,
 and every instance's outflows balance its inflow.
 """
@@ -40,7 +41,8 @@ def _cases():
     return out
 
 
-def test_ensemble_matches_instances_solved_alone():
+@pytest.mark.parametrize("krylov", ["segmented", "union"])
+def test_ensemble_matches_instances_solved_alone(krylov):
     from zvcfd_b200.ensemble import B200Ensemble, solve_sequentially
     from zvcfd_b200.fluid import Fluid
 
@@ -48,7 +50,7 @@ def test_ensemble_matches_instances_solved_alone():
     fl = Fluid(1060.0, 3.5e-3)
     alone = solve_sequentially(cases, fl, tol=1e-9, max_iterations=800, advection=1.0)
     assert all(r["converged"] for r in alone["instances"])
-    ens = B200Ensemble(cases, fl, advection=1.0, linear="b200-mixed",
+    ens = B200Ensemble(cases, fl, krylov=krylov, advection=1.0, linear="b200-mixed",
                        linear_options={"autotune": True})
     rep = ens.solve(tol=1e-9, max_iterations=800)
     assert rep["converged"], rep["history"][-1]

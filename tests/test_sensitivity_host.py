@@ -35,3 +35,42 @@ def test_shear_rate_has_a_zero_slope_at_rest():
     assert float(r[0]) == 0.0 and abs(float(r[1]) - 2.0) < 1e-15
     (g,) = torch.autograd.grad(r.sum(), L)
     assert torch.isfinite(g).all() and float(g[0].abs().max()) == 0.0
+
+
+def test_batched_fgmres_matches_one_solve_per_system():
+    """Lock-step recurrences: each system reaches its own solution; a zero right-hand side
+    takes no steps; a system that converges early freezes while the others go on."""
+    from zvcfd_b200.sensitivity import fgmres, fgmres_batched
+
+    g = torch.Generator().manual_seed(1)
+    n = 150
+    A = 4 * torch.eye(n, dtype=torch.float64) + 0.1 * torch.randn(n, n, generator=g,
+                                                                   dtype=torch.float64)
+    d = torch.diag(A).clone()
+    b = torch.randn(4, n, generator=g, dtype=torch.float64)
+    b[2] = 0.0
+    b[3] = A @ torch.ones(n, dtype=torch.float64) * 1e-3      # an easier system
+    x, its, res = fgmres_batched(lambda v: v @ A.T, b, lambda v: v / d, rtol=1e-12, restart=7)
+    assert (res <= 1e-12).all(), res
+    assert float(x[2].abs().max()) == 0.0
+    for q in (0, 1, 3):
+        ref = torch.linalg.solve(A, b[q])
+        assert torch.linalg.norm(x[q] - ref) <= 1e-11 * torch.linalg.norm(ref)
+        x1, _, _ = fgmres(lambda v: A @ v, b[q], lambda v: v / d, rtol=1e-12, restart=7)
+        assert torch.linalg.norm(x[q] - x1) <= 1e-11 * torch.linalg.norm(ref)
+
+
+def test_rcr_step_restates_the_outlet_model():
+    """The differentiable RCR step is the model's own affine step, trapezoidal and Euler."""
+    from zvcfd_b200.lumped import RCR
+    from zvcfd_b200.sensitivity import rcr_step
+
+    for method in ("trapezoidal", "euler"):
+        m = RCR(rp=1.2e8, c=0.8e-9, rd=1.1e9, pv=0.0, method=method)
+        m.initialise(2e-6, 0.3)
+        m.advance(2.1e-6, 0.301, 1e-3)
+        want = m._affine_step(0.302, 1e-3)
+        t = lambda v: torch.tensor(v, dtype=torch.float64, requires_grad=True)   # noqa: E731
+        got = rcr_step(m, t(m.pc), t(m.q), t(m.rp), t(m.c), t(m.rd), 0.302, 1e-3)
+        assert abs(float(got[0]) - want[0]) <= 1e-12 * abs(want[0])
+        assert abs(float(got[1]) - want[1]) <= 1e-12 * abs(want[1])

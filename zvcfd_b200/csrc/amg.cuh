@@ -14,8 +14,9 @@
 //  * coarse operators: Galerkin with piecewise-constant transfer, the sum of the blocks of
 //    each aggregate pair (linear.py:437-454), in a fixed order (deterministic);
 //  * smoothing: damped block Jacobi with the inverse of each 4x4 diagonal block, symmetric
-//    multicolour block Gauss-Seidel on the finest levels, or block-Jacobi-preconditioned
-//    Chebyshev polynomials (the largest eigenvalue of D^-1 A by power iteration at set-up);
+//    multicolour block Gauss-Seidel or multicolour DILU on the finest levels, or
+//    block-Jacobi-preconditioned Chebyshev polynomials (the largest eigenvalue of D^-1 A by
+//    power iteration at set-up);
 //  * coarsest level: the explicit inverse of the dense matrix (Gauss-Jordan with partial
 //    pivoting in one CTA), or smoothing sweeps when coarsening stalls above that size.
 //
@@ -590,6 +591,157 @@ __global__ void k_fill_start(long long m, T *__restrict__ v) {
     v[i] = (T)(0.5 + (double)(h >> 11) * (1.0 / 9007199254740992.0));
 }
 
+// ------------------------------------------------------------------ multicolour DILU
+
+// Inverse of a 4x4 block by Gauss-Jordan with partial pivoting: false (and inv = 0) if singular.
+__device__ inline bool invert4(const double (&m)[16], double (&inv)[16]) {
+    double a[4][8];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            a[r][c] = m[r * 4 + c];
+            a[r][4 + c] = r == c ? 1.0 : 0.0;
+        }
+    bool ok = true;
+    for (int k = 0; k < 4 && ok; ++k) {
+        int piv = k;
+        for (int r = k + 1; r < 4; ++r)
+            if (fabs(a[r][k]) > fabs(a[piv][k])) piv = r;
+        if (!(fabs(a[piv][k]) > 0.0)) {
+            ok = false;
+            break;
+        }
+        if (piv != k)
+            for (int c = 0; c < 8; ++c) {
+                const double t = a[k][c];
+                a[k][c] = a[piv][c];
+                a[piv][c] = t;
+            }
+        const double s = 1.0 / a[k][k];
+        for (int c = 0; c < 8; ++c) a[k][c] *= s;
+        for (int r = 0; r < 4; ++r) {
+            if (r == k) continue;
+            const double f = a[r][k];
+            if (f != 0.0)
+                for (int c = 0; c < 8; ++c) a[r][c] -= f * a[k][c];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) inv[r * 4 + c] = ok ? a[r][4 + c] : 0.0;
+    return ok;
+}
+
+// The DILU diagonal of one colour, after the earlier colours' (AmgX's MULTICOLOR_DILU, the
+// reference's `dilu` presets, zvcfd/fv/linear.py:571-608):
+//   E_i = A_ii - sum over neighbours j of an earlier colour of A_ij E_j^-1 A_ji,
+// on a colour-ordered level (colour = the contiguous rows [first, first + count); an earlier
+// colour's rows lie below first). The blocks are read in FP64 from the level's own numbering
+// (psrc: the source of every colour-ordered block; ptrans: the colour-ordered position of the
+// transposed block, -1 if absent); E_i^-1 is written in FP64 (a singular E leaves a zero
+// inverse: the row is not smoothed). One thread per row; launched colour by colour in order.
+__global__ void __launch_bounds__(128)
+k_dilu_factor(long long count, long long first, const long long *__restrict__ pptr,
+              const int *__restrict__ pidx, const long long *__restrict__ psrc,
+              const long long *__restrict__ ptrans, const long long *__restrict__ pdpos,
+              const double *__restrict__ data, double *__restrict__ einv) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const long long row = first + k;
+    double E[16];
+    const long long pd = pdpos[row];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) E[e] = pd >= 0 ? data[psrc[pd] * 16 + e] : 0.0;
+    for (long long q = pptr[row]; q < pptr[row + 1]; ++q) {
+        const int j = pidx[q];
+        const long long qt = ptrans[q];
+        if (j >= first || qt < 0) continue;
+        const double *Aij = data + psrc[q] * 16, *Aji = data + psrc[qt] * 16;
+        const double *Ej = einv + (long long)j * 16;
+        double T[16];                                   // T = E_j^-1 A_ji
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                double s = 0.0;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) s += Ej[r * 4 + m] * Aji[m * 4 + c];
+                T[r * 4 + c] = s;
+            }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                double s = 0.0;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) s += Aij[r * 4 + m] * T[m * 4 + c];
+                E[r * 4 + c] -= s;
+            }
+    }
+    double inv[16];
+    invert4(E, inv);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) einv[row * 16 + e] = inv[e];
+}
+
+// One colour of the DILU solve M z = r, M = (E + L) E^-1 (E + U) (L, U: the blocks of earlier
+// and later colours), on a colour-ordered level:
+//   forward (colours in order):     w_i = E_i^-1 (r_i - sum_{j earlier} A_ij w_j)
+//   backward (colours in reverse):  z_i = w_i - E_i^-1 sum_{j later} A_ij z_j,  x_i += omega z_i
+// (w and z share the vector wz). Rows split over G lanes as in the Gauss-Seidel sweep; a lane
+// loads only the blocks on its side of the colour (each pass reads half the level's blocks).
+template <int G, bool BACKWARD, typename V, typename T>
+__global__ void __launch_bounds__(256)
+k_dilu_colour(long long count, long long first, const long long *__restrict__ pptr,
+              const int *__restrict__ pidx, const V *__restrict__ data,
+              const V *__restrict__ einv, const T *__restrict__ r, T *__restrict__ wz,
+              T *__restrict__ x, T omega) {
+    constexpr int S = G / 4;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long k = gid / G;
+    const int lane = threadIdx.x % G;
+    const int slot = lane / 4, rr = lane % 4;
+    const bool on = k < count;
+    const long long row = first + (on ? k : 0);
+    const long long last = first + count;
+    T acc = 0;
+    if (on) {
+        const long long p1 = pptr[row + 1];
+        for (long long p = pptr[row] + slot; p < p1; p += S) {
+            const int j = __ldcs(pidx + p);
+            if (BACKWARD ? j < last : j >= first) continue;
+            const Vec4<V> a = Vec4<V>::load_stream(data + p * 16 + rr * 4);
+            const T *v = wz + (long long)j * 4;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc += (T)a.v[c] * v[c];
+        }
+    }
+#pragma unroll
+    for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    T lhs = 0;
+    if (on) lhs = BACKWARD ? acc : r[row * 4 + rr] - acc;
+    const int base = (threadIdx.x % 32) / G * G;
+    T rc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) rc[c] = __shfl_sync(0xffffffffu, lhs, base + c);
+    if (on && slot == 0) {
+        const Vec4<V> d = Vec4<V>::load(einv + row * 16 + rr * 4);
+        T s = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s += (T)d.v[c] * rc[c];
+        const long long i = row * 4 + rr;
+        if (BACKWARD) {
+            const T z = wz[i] - s;
+            wz[i] = z;
+            x[i] += omega * z;
+        } else {
+            wz[i] = s;
+        }
+    }
+}
+
 // ------------------------------------------------------------------ multicolour Gauss-Seidel
 
 // In-place block Gauss-Seidel over the rows of one colour (rows[0..count)): rows of a colour
@@ -880,6 +1032,7 @@ struct Level {
     long long *pptr = nullptr, *psrc = nullptr, *pdpos = nullptr;   // psrc: source block
     int *pidx = nullptr, *pinv = nullptr;                           // pinv: row -> position
     int *pagg = nullptr, *pmem = nullptr;        // aggregate of each position; members renumbered
+    long long *ptrans = nullptr;                 // DILU: the position of each block's transpose
     double *pdata64 = nullptr, *pdinv64 = nullptr;
     float *pdata32 = nullptr, *pdinv32 = nullptr;
     void *pb = nullptr;                          // the level's right-hand side, colour-ordered
@@ -896,7 +1049,8 @@ struct Level {
 struct Params {
     int precision = 0;       // 0 FP64 cycle, 1 FP32 cycle
     int smoother = 1;        // 0 damped block Jacobi, 1 symmetric multicolour block Gauss-Seidel,
-                             // 2 block-Jacobi-preconditioned Chebyshev (sweeps = degree)
+                             // 2 block-Jacobi-preconditioned Chebyshev (sweeps = degree),
+                             // 3 multicolour DILU on the colour-ordered levels (Jacobi below)
     int gs_levels = 2;       // with Gauss-Seidel: the finest levels that use it (Jacobi below)
     int jacobi_sweeps = 2;   // damped block-Jacobi sweeps (pre and post) below them
     double jacobi_omega = 0.7;

@@ -10,7 +10,9 @@
 // passes over the basis (dots; update + dots; update + norm) with deterministic two-stage
 // reductions, and the Hessenberg matrix, its Givens rotations and the residual estimate stay
 // on the device: the host reads 3 numbers per Krylov step.
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "amg.cuh"
@@ -210,6 +212,210 @@ __global__ void k_lr_axpy(long long m, const long long *__restrict__ ui, const d
                           const double *__restrict__ t, double sign, double *__restrict__ y) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q < m) y[ui[q]] += sign * uv[q] * t[0];
+}
+
+// ------------------------------------------------------------------ segmented Krylov
+//
+// FGMRES with one Krylov recurrence per segment of a block-diagonal system (the instances of
+// an ensemble): the operator and the preconditioner act on all segments at once, every inner
+// product, norm, Hessenberg column, Givens rotation and step length is taken per segment.
+// A pass over the vectors runs one CTA per chunk of a segment: CTA c covers the entries
+// [cfirst[c], cfirst[c + 1]) of segment cseg[c], and the CTAs of segment s are
+// sfirst[s] .. sfirst[s + 1] - 1, so that a segment's sums fold over its own CTAs in a fixed
+// order. Per-segment arrays are strided by MAXV (h, norms, y), by ldh (rotations) or by
+// ldh * ldh (Hessenberg), ldh = restart + 1.
+
+// MODE 0: partial[c][j] = (V_j . w) over the CTA's chunk, j < nv; 1: w -= sum_j h[s][j] V_j
+// first, then the dots; 2: the update, then partial[c][0] = |w|^2; 3: |w|^2 alone (w unchanged)
+template <int MODE>
+__global__ void __launch_bounds__(DOT_THREADS)
+k_seg_pass(const long long *__restrict__ cfirst, const int *__restrict__ cseg,
+           const double *__restrict__ V, long long ldv, int nv, const double *__restrict__ h,
+           double *__restrict__ w, double *__restrict__ partial) {
+    constexpr bool UPDATE = MODE == 1 || MODE == 2;
+    constexpr bool DOTS = MODE < 2;
+    const int c = blockIdx.x;
+    const long long i0 = cfirst[c], i1 = cfirst[c + 1];
+    __shared__ double hs[MAXV];
+    if (UPDATE && threadIdx.x < MAXV)
+        hs[threadIdx.x] = (int)threadIdx.x < nv ? h[(long long)cseg[c] * MAXV + threadIdx.x] : 0.0;
+    __syncthreads();
+    double acc[MAXV];
+#pragma unroll
+    for (int j = 0; j < MAXV; ++j) acc[j] = 0.0;
+    for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        double wi = w[i];
+        if (UPDATE) {
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < MAXV; ++j)
+                if (j < nv) s += hs[j] * V[j * ldv + i];
+            wi -= s;
+            w[i] = wi;
+        }
+        if (DOTS) {
+#pragma unroll
+            for (int j = 0; j < MAXV; ++j)
+                if (j < nv) acc[j] += V[j * ldv + i] * wi;
+        } else {
+            acc[0] += wi * wi;
+        }
+    }
+    __shared__ double red[DOT_THREADS / 32][MAXV];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int cols = DOTS ? nv : 1;
+#pragma unroll
+    for (int j = 0; j < MAXV; ++j)
+        if (j < cols) {
+            const double v = warp_sum(acc[j]);
+            if (lane == 0) red[warp][j] = v;
+        }
+    __syncthreads();
+    if ((int)threadIdx.x < cols) {
+        double v = 0.0;
+        for (int q = 0; q < DOT_THREADS / 32; ++q) v += red[q][threadIdx.x];
+        partial[(long long)c * MAXV + threadIdx.x] = v;
+    }
+}
+
+// out[s][j] = sum over segment s's CTAs of partial[c][j] (one CTA of 32 * MAXV threads per
+// segment, a warp per column: lane-strided sums, then a fixed butterfly); 0 for no CTAs
+__global__ void k_seg_fold(const int *__restrict__ sfirst, int cols, const double *__restrict__ partial,
+                           double *__restrict__ out) {
+    const int s = blockIdx.x, j = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (j >= cols) return;
+    double v = 0.0;
+    for (int c = sfirst[s] + lane; c < sfirst[s + 1]; c += 32) v += partial[(long long)c * MAXV + j];
+    v = warp_sum(v);
+    if (lane == 0) out[(long long)s * MAXV + j] = v;
+}
+
+// per segment at the start of a solve: beta0 = |r|, target = max(rtol beta0, 1e-13 |b|)
+// (the floor of the single-recurrence solve); bb, rr: folded squares (MAXV-strided)
+__global__ void k_seg_targets(int nseg, double rtol, const double *__restrict__ bb,
+                              const double *__restrict__ rr, double *__restrict__ beta0,
+                              double *__restrict__ target) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    const double b0 = sqrt(rr[(long long)s * MAXV]);
+    beta0[s] = b0;
+    target[s] = fmax(rtol * b0, 1e-13 * sqrt(bb[(long long)s * MAXV]));
+}
+
+// a restart cycle's first column: g = (beta, 0, ...), the segment active (kk = -1) while its
+// residual is above target, else frozen with no steps (kk = 0); inv = 1 / beta when active.
+// active: the number of active segments (zeroed by the caller)
+__global__ void k_seg_init(int nseg, int ldh, const double *__restrict__ rr,
+                           const double *__restrict__ target, double *__restrict__ g,
+                           int *__restrict__ kk, double *__restrict__ inv, int *__restrict__ active) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    const double beta = sqrt(rr[(long long)s * MAXV]);
+    double *gs = g + (long long)s * (ldh + 1);
+    for (int i = 0; i <= ldh; ++i) gs[i] = i == 0 ? beta : 0.0;
+    const bool on = beta > target[s];
+    kk[s] = on ? -1 : 0;
+    inv[s * 4 + 2] = on && beta > 0.0 ? 1.0 / beta : 0.0;
+    if (on) atomicAdd(active, 1);
+}
+
+// column k of each active segment's Hessenberg matrix (the per-segment form of
+// k_arnoldi_finish); a segment that reaches its target or breaks down (h_{k+1,k} = 0) freezes
+// with kk = k + 1 steps. st[s]: [0] |g[k+1]|, [1] h_{k+1,k}, [2] the scale of the next basis
+// vector (0 once frozen). active: segments still active after this step.
+__global__ void k_seg_finish(int k, int nseg, int ldh, const double *__restrict__ h1,
+                             const double *__restrict__ h2, const double *__restrict__ nrm2,
+                             const double *__restrict__ target, double *__restrict__ H,
+                             double *__restrict__ cs, double *__restrict__ sn, double *__restrict__ g,
+                             int *__restrict__ kk, double *__restrict__ st, int *__restrict__ active) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    double *sts = st + (long long)s * 4;
+    if (kk[s] >= 0) {
+        sts[2] = 0.0;
+        return;
+    }
+    const double *a = h1 + (long long)s * MAXV, *b = h2 + (long long)s * MAXV;
+    double *col = H + (long long)s * ldh * ldh + (long long)k * ldh;
+    double *c = cs + (long long)s * ldh, *sv = sn + (long long)s * ldh;
+    double *gs = g + (long long)s * (ldh + 1);
+    for (int j = 0; j <= k; ++j) col[j] = a[j] + b[j];
+    const double hn = sqrt(nrm2[(long long)s * MAXV]);
+    col[k + 1] = hn;
+    for (int j = 0; j < k; ++j) {
+        const double t = c[j] * col[j] + sv[j] * col[j + 1];
+        col[j + 1] = -sv[j] * col[j] + c[j] * col[j + 1];
+        col[j] = t;
+    }
+    const double den = hypot(col[k], col[k + 1]);
+    if (den != 0.0) {
+        c[k] = col[k] / den;
+        sv[k] = col[k + 1] / den;
+    } else {
+        c[k] = 1.0;
+        sv[k] = 0.0;
+    }
+    col[k] = den;
+    col[k + 1] = 0.0;
+    gs[k + 1] = -sv[k] * gs[k];
+    gs[k] = c[k] * gs[k];
+    sts[0] = fabs(gs[k + 1]);
+    sts[1] = hn;
+    // frozen: at its target, or a breakdown - a vanished h_{k+1,k} (the space holds the
+    // solution: keep the column), or a vanished rotated diagonal (drop the column)
+    const bool done = sts[0] <= target[s] || hn == 0.0 || den == 0.0;
+    sts[2] = done ? 0.0 : 1.0 / hn;
+    if (done) kk[s] = den == 0.0 ? k : k + 1;
+    else atomicAdd(active, 1);
+}
+
+// out[i] = a[i] * sc[cseg(i) * 4 + 2]: a basis vector scaled per segment
+__global__ void k_seg_scale(const long long *__restrict__ cfirst, const int *__restrict__ cseg,
+                            const double *__restrict__ a, const double *__restrict__ sc,
+                            double *__restrict__ out) {
+    const int c = blockIdx.x;
+    const double f = sc[(long long)cseg[c] * 4 + 2];
+    for (long long i = cfirst[c] + threadIdx.x; i < cfirst[c + 1]; i += blockDim.x) out[i] = a[i] * f;
+}
+
+// y[s] = H_s(0:K, 0:K)^-1 g_s, K = the segment's steps (kk, or ku while still active);
+// y[s][j] = 0 for j >= K
+__global__ void k_seg_upper(int nseg, int ku, int ldh, const double *__restrict__ H,
+                            const double *__restrict__ g, const int *__restrict__ kk,
+                            double *__restrict__ y) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    const int K = kk[s] < 0 ? ku : kk[s];
+    const double *Hs = H + (long long)s * ldh * ldh, *gs = g + (long long)s * (ldh + 1);
+    double *ys = y + (long long)s * MAXV;
+    for (int j = K; j < MAXV; ++j) ys[j] = 0.0;
+    for (int i = K - 1; i >= 0; --i) {
+        double v = gs[i];
+        for (int j = i + 1; j < K; ++j) v -= Hs[(long long)j * ldh + i] * ys[j];
+        ys[i] = v / Hs[(long long)i * ldh + i];
+    }
+}
+
+// x += sum_j y[s][j] Z_j over each segment's entries (j < ku; y is 0 past a segment's steps)
+__global__ void k_seg_combine(const long long *__restrict__ cfirst, const int *__restrict__ cseg,
+                              const double *__restrict__ Z, long long ldz, int ku,
+                              const double *__restrict__ y, double *__restrict__ x) {
+    const int c = blockIdx.x;
+    __shared__ double ys[MAXV];
+    if (threadIdx.x < MAXV) ys[threadIdx.x] = (int)threadIdx.x < ku ? y[(long long)cseg[c] * MAXV + threadIdx.x] : 0.0;
+    __syncthreads();
+    for (long long i = cfirst[c] + threadIdx.x; i < cfirst[c + 1]; i += blockDim.x) {
+        double v = 0.0;
+        for (int j = 0; j < ku; ++j) v += ys[j] * Z[j * ldz + i];
+        x[i] += v;
+    }
+}
+
+// the segments whose residual (folded squares rr) is above target
+__global__ void k_seg_open(int nseg, const double *__restrict__ rr, const double *__restrict__ target,
+                           int *__restrict__ open) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nseg && sqrt(rr[(long long)s * MAXV]) > target[s]) atomicAdd(open, 1);
 }
 
 struct LowRank {
@@ -599,6 +805,27 @@ class Hierarchy {
                                            cudaMemcpyHostToDevice, st), "colouring: sources"));
         ZV_TRY(cuda_status(cudaMemcpyAsync(ddpos, pdpos.data(), n * sizeof(long long),
                                            cudaMemcpyHostToDevice, st), "colouring: diagonal"));
+        if (prm.smoother == 3) {
+            // the transposed block of every colour-ordered block: (j, i) is found in the sorted
+            // original row j, and keeps its place there in the colour-ordered row
+            std::vector<long long> ptr_t(nnz, -1);
+            for (long long k = 0; k < n; ++k) {
+                const long long i0 = order[k];
+                for (long long p = ip[i0]; p < ip[i0 + 1]; ++p) {
+                    const int jj = ix[p];
+                    const int *lo = ix.data() + ip[jj], *hi = ix.data() + ip[jj + 1];
+                    const int *f = std::lower_bound(lo, hi, (int)i0);
+                    if (f != hi && *f == (int)i0)
+                        ptr_t[pptr[k] + (p - ip[i0])] = pptr[inv[jj]] + (f - lo);
+                }
+            }
+            long long *dt;
+            ZV_TRY(keep.get(&dt, nnz));
+            ZV_TRY(cuda_status(cudaMemcpyAsync(dt, ptr_t.data(), nnz * sizeof(long long),
+                                               cudaMemcpyHostToDevice, st), "colouring: transposes"));
+            ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colouring: transposes"));
+            v.ptrans = dt;
+        }
         ZV_TRY(cuda_status(cudaStreamSynchronize(st), "colouring: upload"));
         v.gs_rows = rows;
         v.pinv = dinv_;
@@ -618,7 +845,7 @@ class Hierarchy {
             k_diag_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.indices, nullptr, nullptr,
                                                           v.dpos); count_launch();
             k_rows_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.rows); count_launch();
-            if (prm.smoother == 1 && v.n > DENSE_MAX && (int)l < prm.gs_levels) {
+            if ((prm.smoother == 1 || prm.smoother == 3) && v.n > DENSE_MAX && (int)l < prm.gs_levels) {
                 if (l == 0 && coloured_indptr == v.indptr && coloured_n == v.n &&
                     coloured_nnz == v.nnz && c0.gs_rows) {
                     // the finest pattern does not change: its colouring and colour order stay
@@ -629,6 +856,7 @@ class Hierarchy {
                     v.psrc = c0.psrc;
                     v.pdpos = c0.pdpos;
                     v.pinv = c0.pinv;
+                    v.ptrans = c0.ptrans;
                 } else {
                     if (l == 0) persist.release();
                     ZV_TRY(colour_level(v, l == 0 ? persist : structure));
@@ -753,6 +981,7 @@ class Hierarchy {
                     k_permute_rows<true, double, double><<<gd, 256, 0, st>>>(v.n, 16, v.gs_rows, v.dinv64, v.pdinv64); count_launch();
                 }
             }
+            if (v.pptr && prm.smoother == 3) ZV_TRY(dilu_factor(v));
             // FP32 copies in the original numbering: every level but the Gauss-Seidel ones
             // (which sweep their colour-ordered copy), and those too once A^T is solved with
             if (prm.precision == 1 && (!v.pptr || transposed_used)) ZV_TRY(convert_original(v));
@@ -780,6 +1009,26 @@ class Hierarchy {
             }
         }
         return launch_status("hierarchy values");
+    }
+
+    // the DILU inverses of a colour-ordered level, colour by colour, in FP64 (into the level's
+    // colour-ordered inverses, converted for the FP32 hierarchy)
+    int dilu_factor(Level &v) {
+        double *e = v.pdinv64;
+        if (prm.precision == 1) ZV_TRY(scratch.get(&e, v.n * 16));
+        const int C = (int)v.gs_off.size() - 1;
+        for (int c = 0; c < C; ++c) {
+            const long long o = v.gs_off[c], cnt = v.gs_off[c + 1] - o;
+            if (cnt <= 0) continue;
+            k_dilu_factor<<<grid_for(cnt, 128), 128, 0, st>>>(cnt, o, v.pptr, v.pidx, v.psrc, v.ptrans,
+                                                               v.pdpos, v.data, e); count_launch();
+        }
+        if (prm.precision == 1) {
+            k_convert<double, float><<<grid_for(v.n * 16, 256), 256, 0, st>>>(v.n * 16, e, v.pdinv32); count_launch();
+            ZV_TRY(launch_status("dilu factor"));
+            scratch.release();
+        }
+        return launch_status("dilu factor");
     }
 
     int convert_original(Level &v) {
@@ -927,6 +1176,38 @@ void gs_pass(const Level &v, const V *data, const V *dinv, const T *b, T *x, T o
     }
 }
 
+// one DILU smoothing step on a colour-ordered level: r = b - A x (b itself while x is the zero
+// start), the forward solve over the colours into w, the backward solve over them with
+// x += omega z (k_dilu_colour)
+template <typename V, typename T>
+void dilu_sweep(const Level &v, const V *data, const V *einv, const T *b, T *x, T *r, T *w, T omega,
+                bool x_zero, cudaStream_t st) {
+    const T *rr = b;
+    if (!x_zero) {
+        bsr_spmv_launch<true, V, T>(v.lanes, v.n, v.pptr, v.pidx, data, x, b, r, st);
+        rr = r;
+    }
+    const int C = (int)v.gs_off.size() - 1;
+    const int G = v.lanes;
+    for (int back = 0; back < 2; ++back)
+        for (int q = 0; q < C; ++q) {
+            const int c = back ? C - 1 - q : q;
+            const long long o = v.gs_off[c], cnt = v.gs_off[c + 1] - v.gs_off[c];
+            if (cnt <= 0) continue;
+            const unsigned grid = grid_for(cnt * G, 256);
+            if (back) {
+                if (G == 8) k_dilu_colour<8, true, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+                else if (G == 16) k_dilu_colour<16, true, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+                else k_dilu_colour<32, true, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+            } else {
+                if (G == 8) k_dilu_colour<8, false, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+                else if (G == 16) k_dilu_colour<16, false, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+                else k_dilu_colour<32, false, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+            }
+            count_launch();
+        }
+}
+
 template <typename T>
 struct CyclePick;
 template <>
@@ -961,8 +1242,9 @@ int Hierarchy::cycle(size_t l) {
     const auto *data = CyclePick<T>::data(v);
     const auto *dinv = CyclePick<T>::dinv(v);
     using V = typename std::remove_const<typename std::remove_pointer<decltype(data)>::type>::type;
-    const bool gs_level = prm.smoother == 1 && !v.gs_off.empty();
-    const bool jac_below = prm.smoother == 1 && !gs_level;       // Jacobi below the GS levels
+    const bool coloured = prm.smoother == 1 || prm.smoother == 3;
+    const bool gs_level = coloured && !v.gs_off.empty();
+    const bool jac_below = coloured && !gs_level;       // Jacobi below the GS / DILU levels
     const T omega = (T)(jac_below ? prm.jacobi_omega : prm.omega);
     const bool last = (l + 1 == L.size()) || v.agg == nullptr;
     const int pre = last ? prm.coarse_sweeps : (jac_below ? prm.jacobi_sweeps : prm.presweeps);
@@ -976,7 +1258,13 @@ int Hierarchy::cycle(size_t l) {
         const unsigned g4 = grid_for(v.n * 4, 256);
         k_permute_rows<true, T, T><<<g4, 256, 0, st>>>(v.n, 4, v.gs_rows, b, pb); count_launch();
         cudaMemsetAsync(px, 0, v.n * 4 * sizeof(T), st);
+        bool zero = true;                 // px is still the zero start
         auto sgs = [&](int sweeps) {      // symmetric: forward then backward over the colours
+            if (prm.smoother == 3) {
+                for (int s = 0; s < sweeps; ++s, zero = false)
+                    dilu_sweep<V, T>(v, pdata, pdinv, pb, px, pr, static_cast<T *>(v.x), omega, zero, st);
+                return;
+            }
             for (int s = 0; s < sweeps; ++s) {
                 gs_pass<false, V, T>(v, pdata, pdinv, pb, px, omega, false, st);
                 gs_pass<false, V, T>(v, pdata, pdinv, pb, px, omega, true, st);
@@ -989,6 +1277,7 @@ int Hierarchy::cycle(size_t l) {
             k_restrict<T><<<grid_for(c.n * 4, 256), 256, 0, st>>>(c.n, v.mptr, v.pmem, pr, static_cast<T *>(c.b)); count_launch();
             ZV_TRY((cycle<T, TRANS>(l + 1)));
             k_prolong_add<T><<<g4, 256, 0, st>>>(v.n, v.pagg, static_cast<const T *>(c.x), px); count_launch();
+            zero = false;
             sgs(prm.postsweeps);
         }
         k_permute_rows<false, T, T><<<g4, 256, 0, st>>>(v.n, 4, v.gs_rows, px, static_cast<T *>(v.x)); count_launch();
@@ -1345,6 +1634,171 @@ struct Solver {
         ZV_TRY(launch_status("fgmres"));
         return std::isfinite(res) ? OK : NON_FINITE;
     }
+
+    // ---- segmented FGMRES (one recurrence per segment; kernels above)
+    Arena segwork;
+    std::vector<long long> seg_rows;       // the segment bounds the buffers below were built for
+    int nseg = 0, nsc = 0;                 // segments, CTAs of a segmented pass
+    long long seg_n4 = 0;
+    long long *cfirst = nullptr;
+    int *cseg = nullptr, *sfirst = nullptr, *kk = nullptr, *cnt = nullptr;
+    double *spart = nullptr, *sh1 = nullptr, *sh2 = nullptr, *snrm = nullptr, *sbb = nullptr;
+    double *srr = nullptr, *sbeta0 = nullptr, *starget = nullptr, *sH = nullptr, *scs = nullptr;
+    double *ssn = nullptr, *sg = nullptr, *sy = nullptr, *sst = nullptr, *sinv = nullptr;
+
+    int ensure_segments(int ns, const long long *rows) {
+        std::vector<long long> want(rows, rows + ns + 1);
+        if (want == seg_rows && cfirst && seg_n4 == n4) return OK;
+        for (int q = 0; q < ns; ++q)
+            if (want[q + 1] < want[q]) {
+                set_error("solve_segmented: segment bounds must not decrease");
+                return BAD_ARGUMENT;
+            }
+        if (want[0] != 0 || want[ns] != n) {
+            set_error("solve_segmented: segments must cover rows 0 to %lld", (long long)n);
+            return BAD_ARGUMENT;
+        }
+        segwork.set_stream(st);
+        segwork.release();
+        seg_rows = want;
+        seg_n4 = n4;
+        nseg = ns;
+        // chunks of at least 2048 entries, about four CTAs per SM over the whole vector
+        long long chunk = (n4 + 4LL * sm_count() - 1) / (4LL * sm_count());
+        chunk = std::max<long long>(2048, (chunk + 255) / 256 * 256);
+        std::vector<long long> cf;
+        std::vector<int> cs_, sf(ns + 1);
+        for (int q = 0; q < ns; ++q) {
+            sf[q] = (int)cs_.size();
+            for (long long a = 4 * want[q]; a < 4 * want[q + 1]; a += chunk) {
+                cf.push_back(a);
+                cs_.push_back(q);
+            }
+        }
+        sf[ns] = (int)cs_.size();
+        cf.push_back(n4);
+        nsc = (int)cs_.size();
+        const int ldh = restart + 1;
+        ZV_TRY(segwork.get(&cfirst, cf.size()));
+        ZV_TRY(segwork.get(&cseg, std::max(nsc, 1)));
+        ZV_TRY(segwork.get(&sfirst, ns + 1));
+        ZV_TRY(segwork.get(&kk, ns));
+        ZV_TRY(segwork.get(&cnt, 1));
+        ZV_TRY(segwork.get(&spart, (size_t)std::max(nsc, 1) * MAXV));
+        for (double **q : {&sh1, &sh2, &snrm, &sbb, &srr, &sy}) ZV_TRY(segwork.get(q, (size_t)ns * MAXV));
+        ZV_TRY(segwork.get(&sbeta0, ns));
+        ZV_TRY(segwork.get(&starget, ns));
+        ZV_TRY(segwork.get(&sH, (size_t)ns * ldh * ldh));
+        ZV_TRY(segwork.get(&scs, (size_t)ns * ldh));
+        ZV_TRY(segwork.get(&ssn, (size_t)ns * ldh));
+        ZV_TRY(segwork.get(&sg, (size_t)ns * (ldh + 1)));
+        ZV_TRY(segwork.get(&sst, (size_t)ns * 4));
+        ZV_TRY(segwork.get(&sinv, (size_t)ns * 4));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(cfirst, cf.data(), cf.size() * sizeof(long long),
+                                           cudaMemcpyHostToDevice, st), "segments"));
+        if (nsc)
+            ZV_TRY(cuda_status(cudaMemcpyAsync(cseg, cs_.data(), nsc * sizeof(int),
+                                               cudaMemcpyHostToDevice, st), "segments"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(sfirst, sf.data(), (ns + 1) * sizeof(int),
+                                           cudaMemcpyHostToDevice, st), "segments"));
+        // the pageable host vectors above must outlive the copies
+        return cuda_status(cudaStreamSynchronize(st), "segments");
+    }
+
+    // |v|^2 per segment into out (MAXV-strided)
+    void seg_norm2(const double *v, double *out) {
+        k_seg_pass<3><<<nsc, DOT_THREADS, 0, st>>>(cfirst, cseg, nullptr, 0, 0, nullptr,
+                                                   const_cast<double *>(v), spart); count_launch();
+        k_seg_fold<<<nseg, 32 * MAXV, 0, st>>>(sfirst, 1, spart, out); count_launch();
+    }
+
+    int read_count(const char *what, int *out) {
+        ZV_TRY(cuda_status(cudaMemcpyAsync(host, cnt, sizeof(int), cudaMemcpyDeviceToHost, st), what));
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), what));
+        std::memcpy(out, host, sizeof(int));
+        return OK;
+    }
+
+    int solve_segmented(int ns, const long long *rows, const double *b, double *xio, double rtol,
+                        int maxiter, const std::vector<LowRank> &lr, int *iterations,
+                        double *residuals, int *converged) {
+        ZV_TRY(ensure_segments(ns, rows));
+        if (nsc == 0) {
+            *iterations = 0;
+            for (int q = 0; q < ns; ++q) {
+                residuals[q] = 0.0;
+                converged[q] = 1;
+            }
+            return OK;
+        }
+        const int m = restart, ldh = m + 1;
+        const unsigned gs = grid_for(ns, 128);
+        cudaMemcpyAsync(x, xio, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        ZV_TRY(apply(x, b, r, lr));
+        seg_norm2(b, sbb);
+        seg_norm2(r, srr);
+        k_seg_targets<<<gs, 128, 0, st>>>(ns, rtol, sbb, srr, sbeta0, starget); count_launch();
+        int it = 0, open = 0;
+        while (it < maxiter) {
+            cudaMemsetAsync(cnt, 0, sizeof(int), st);
+            k_seg_init<<<gs, 128, 0, st>>>(ns, ldh, srr, starget, sg, kk, sinv, cnt); count_launch();
+            ZV_TRY(read_count("segmented start", &open));
+            if (open == 0) break;
+            k_seg_scale<<<nsc, 256, 0, st>>>(cfirst, cseg, r, sinv, V); count_launch();
+            int ku = 0;
+            for (int k = 0; k < m; ++k) {
+                double *vk = V + (size_t)k * n4, *zk = Z + (size_t)k * n4;
+                ZV_TRY(precondition(vk, zk));
+                ZV_TRY(apply(zk, nullptr, w, lr));
+                const int nv = k + 1;
+                k_seg_pass<0><<<nsc, DOT_THREADS, 0, st>>>(cfirst, cseg, V, n4, nv, nullptr, w, spart); count_launch();
+                k_seg_fold<<<ns, 32 * MAXV, 0, st>>>(sfirst, nv, spart, sh1); count_launch();
+                k_seg_pass<1><<<nsc, DOT_THREADS, 0, st>>>(cfirst, cseg, V, n4, nv, sh1, w, spart); count_launch();
+                k_seg_fold<<<ns, 32 * MAXV, 0, st>>>(sfirst, nv, spart, sh2); count_launch();
+                k_seg_pass<2><<<nsc, DOT_THREADS, 0, st>>>(cfirst, cseg, V, n4, nv, sh2, w, spart); count_launch();
+                k_seg_fold<<<ns, 32 * MAXV, 0, st>>>(sfirst, 1, spart, snrm); count_launch();
+                cudaMemsetAsync(cnt, 0, sizeof(int), st);
+                k_seg_finish<<<gs, 128, 0, st>>>(k, ns, ldh, sh1, sh2, snrm, starget, sH, scs, ssn, sg,
+                                                 kk, sst, cnt); count_launch();
+                ZV_TRY(launch_status("segmented arnoldi"));
+                ZV_TRY(read_count("segmented step", &open));
+                ++it;
+                ku = k + 1;
+                if (open == 0 || it >= maxiter) break;
+                k_seg_scale<<<nsc, 256, 0, st>>>(cfirst, cseg, w, sst, V + (size_t)(k + 1) * n4); count_launch();
+            }
+            k_seg_upper<<<gs, 128, 0, st>>>(ns, ku, ldh, sH, sg, kk, sy); count_launch();
+            k_seg_combine<<<nsc, 256, 0, st>>>(cfirst, cseg, Z, n4, ku, sy, x); count_launch();
+            ZV_TRY(apply(x, b, r, lr));
+            seg_norm2(r, srr);
+            cudaMemsetAsync(cnt, 0, sizeof(int), st);
+            k_seg_open<<<gs, 128, 0, st>>>(ns, srr, starget, cnt); count_launch();
+            ZV_TRY(read_count("segmented restart", &open));
+            if (open == 0) break;
+        }
+        // per segment: |r| / beta0 and whether |r| <= 1.01 target
+        std::vector<double> rr((size_t)ns * MAXV), b0(ns), tg(ns);
+        ZV_TRY(cuda_status(cudaMemcpyAsync(rr.data(), srr, rr.size() * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st), "segmented result"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(b0.data(), sbeta0, ns * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st), "segmented result"));
+        ZV_TRY(cuda_status(cudaMemcpyAsync(tg.data(), starget, ns * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st), "segmented result"));
+        cudaMemcpyAsync(xio, x, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        ZV_TRY(cuda_status(cudaStreamSynchronize(st), "segmented result"));
+        bool all = true, finite = true;
+        for (int q = 0; q < ns; ++q) {
+            const double rn = std::sqrt(rr[(size_t)q * MAXV]);
+            residuals[q] = b0[q] > 0.0 ? rn / b0[q] : rn;
+            converged[q] = rn <= 1.01 * tg[q] ? 1 : 0;
+            all = all && converged[q];
+            finite = finite && std::isfinite(rn);
+        }
+        *iterations = it;
+        H.record_solve(it, all);
+        ZV_TRY(launch_status("segmented fgmres"));
+        return finite ? OK : NON_FINITE;
+    }
 };
 
 }  // namespace
@@ -1396,7 +1850,7 @@ extern "C" {
 int zvfv_solver_create(void **handle, int precision, int smoother, int strength, int passes,
                        int presweeps, int postsweeps, double omega, int coarse_sweeps,
                        int max_levels, int rebuild_every, int restart) {
-    if (!handle || precision < 0 || precision > 1 || smoother < 0 || smoother > 2 || restart < 1 ||
+    if (!handle || precision < 0 || precision > 1 || smoother < 0 || smoother > 3 || restart < 1 ||
         restart > MAXV - 1 || passes < 1 || presweeps < 1 || postsweeps < 0 || max_levels < 1) {
         set_error("solver_create: bad arguments");
         return BAD_ARGUMENT;
@@ -1452,6 +1906,34 @@ int zvfv_solver_solve(void *handle, const double *b, double *x, double rtol, int
         lr.push_back({(const long long *)u_idx[q], u_val[q], (long long)u_len[q],
                       (const long long *)w_idx[q], w_val[q], (long long)w_len[q]});
     return s->solve(b, x, rtol, maxiter, lr, iterations, residual, converged);
+}
+
+// FGMRES with one Krylov recurrence per segment of rows (row_bounds: n_segments + 1
+// ascending host values from 0 to n): the block-diagonal system of independent instances.
+// Each segment stops at its own target, rtol times its initial residual (floor 1e-13 |b_s|);
+// the solve ends when every segment has, or after maxiter Krylov steps (shared by all).
+// residuals / converged: n_segments host values (relative residual, 0/1).
+int zvfv_solver_solve_segmented(void *handle, int n_segments, const int64_t *row_bounds,
+                                const double *b, double *x, double rtol, int maxiter,
+                                int n_lowrank, const int64_t *const *u_idx,
+                                const double *const *u_val, const int64_t *u_len,
+                                const int64_t *const *w_idx, const double *const *w_val,
+                                const int64_t *w_len, int *iterations, double *residuals,
+                                int *converged, void *stream) {
+    Solver *s = static_cast<Solver *>(handle);
+    if (!s || !s->data || !b || !x || maxiter < 0 || n_segments < 1 || !row_bounds || !iterations ||
+        !residuals || !converged) {
+        set_error("solver_solve_segmented: not set up or bad arguments");
+        return BAD_ARGUMENT;
+    }
+    s->st = as_stream(stream);
+    s->H.st = s->st;
+    std::vector<LowRank> lr;
+    for (int q = 0; q < n_lowrank; ++q)
+        lr.push_back({(const long long *)u_idx[q], u_val[q], (long long)u_len[q],
+                      (const long long *)w_idx[q], w_val[q], (long long)w_len[q]});
+    return s->solve_segmented(n_segments, (const long long *)row_bounds, b, x, rtol, maxiter, lr,
+                              iterations, residuals, converged);
 }
 
 // the adjoint solve: A^T x = b with the same hierarchy, transposed (same arguments)
@@ -1535,8 +2017,22 @@ int zvfv_solver_smooth(void *handle, int level, int passes, void *stream) {
         return launch_status("solver_smooth");
     }
     if (v.gs_off.empty() || !v.pb || !v.x2) {
-        set_error("solver_smooth: level %d is not smoothed by Gauss-Seidel or Chebyshev", level);
+        set_error("solver_smooth: level %d is not smoothed by Gauss-Seidel, DILU or Chebyshev",
+                  level);
         return BAD_ARGUMENT;
+    }
+    if (s->H.prm.smoother == 3) {            // DILU steps (residual, forward, backward)
+        for (int q = 0; q < passes; ++q) {
+            if (s->H.prm.precision == 1)
+                dilu_sweep<float, float>(v, v.pdata32, v.pdinv32, static_cast<const float *>(v.pb),
+                                         static_cast<float *>(v.x2), static_cast<float *>(v.r),
+                                         static_cast<float *>(v.x), (float)s->H.prm.omega, false, st);
+            else
+                dilu_sweep<double, double>(v, v.pdata64, v.pdinv64, static_cast<const double *>(v.pb),
+                                           static_cast<double *>(v.x2), static_cast<double *>(v.r),
+                                           static_cast<double *>(v.x), s->H.prm.omega, false, st);
+        }
+        return launch_status("solver_smooth");
     }
     for (int q = 0; q < passes; ++q) {
         if (s->H.prm.precision == 1)

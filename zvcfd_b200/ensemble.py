@@ -15,10 +15,15 @@ have converged with the last linear solve converged.
 The reference solves instances one after the other; :func:`solve_sequentially` is that
 baseline on the same GPU.
 
-Limitation: FGMRES runs over the union, so its inner products and its residual reduction are
-those of all instances together. Instances of similar size and residual converge together (the
-three-vessel test); on the 12-vessel workload (59k-909k nodes) the small instances get no
-reduction of their own and nothing converges. Per-instance Krylov recurrences would be needed.
+The linear solve has two forms. ``krylov="union"`` runs one FGMRES over the union, so its
+inner products and its residual reduction are those of all instances together: instances of
+similar size and residual converge together (the three-vessel test), but on the 12-vessel
+workload (59k-909k nodes) the small instances get no reduction of their own.
+``krylov="segmented"`` (the default) runs one Krylov recurrence per instance inside the device
+FGMRES (``zvfv_solver_solve_segmented``): the operator products and V-cycles still cover all
+instances in one launch each, while every inner product, Hessenberg column, rotation and step
+length is per instance, and each instance's solve stops at ``linear_rtol`` of its own initial
+residual. :func:`segmented_fgmres` restates that algorithm in torch (checked on the CPU).
 """
 
 from __future__ import annotations
@@ -139,46 +144,11 @@ def segmented_fgmres(apply_A, apply_M, b, x0, bounds, rtol: float, *, restart: i
     return x, its, float(rel.max()), bool((beta <= 1.01 * target).all())
 
 
-class SegmentedKrylov:
-    """A linear back end for the ensemble's union system: the AMG hierarchy of ``amg`` (built
-    on the union: block-diagonal, since its aggregates never cross instances) preconditions
-    :func:`segmented_fgmres` with one Krylov recurrence per instance (``krylov="segmented"``).
-
-    Experimental: the recurrences run as torch operations (a few launches per instance and a
-    host read-back per Krylov step); an earlier form, with launches growing with the Krylov
-    index, exceeded 200 s on the three-vessel ensemble test; the algorithm is checked on the
-    CPU. It is the shape of the per-instance recurrences the union solve needs, to be moved
-    into the device FGMRES."""
-
-    name = "b200-segmented"
-
-    def __init__(self, offsets, amg, *, restart: int = 30, maxiter: int = 200):
-        self.amg, self.restart, self.maxiter = amg, restart, maxiter
-        self.bounds = [4 * int(o) for o in offsets]
-        self.rtol = amg.rtol
-
-    def solve(self, A, b, x0=None, rtol=None):
-        from zvcfd_b200.linear import SolveInfo
-
-        ts = self.amg.setup(A)
-        t = time.time()
-        b = b.reshape(-1).contiguous()
-        x0 = torch.zeros_like(b) if x0 is None else x0.reshape(-1).contiguous()
-        x, its, res, ok = segmented_fgmres(A.matvec, self.amg.vcycle, b, x0, self.bounds,
-                                           self.rtol if rtol is None else rtol,
-                                           restart=self.restart, maxiter=self.maxiter)
-        torch.cuda.synchronize()
-        return x, SolveInfo(its, res, time.time() - t, ts, ok)
-
-    def close(self):
-        self.amg.close()
-
-
 class B200Ensemble:
     """Independent steady problems ``cases = [(mesh, bcs), ...]`` of one fluid, solved together
     (see the module docstring). ``solver_options`` go to :class:`B200Solver`."""
 
-    def __init__(self, cases: list, fluid, *, krylov: str = "union", **solver_options):
+    def __init__(self, cases: list, fluid, *, krylov: str = "segmented", **solver_options):
         meshes = [m for m, _ in cases]
         self.mesh, self.offsets, self.zone_ids = union(meshes)
         bcs = {}
@@ -190,11 +160,13 @@ class B200Ensemble:
             from zvcfd_b200.linear import B200AMG
 
             lin = solver_options.pop("linear", "b200")
+            if lin not in ("b200", "b200-mixed"):
+                raise ValueError(f"krylov 'segmented' builds its own b200 back end, not {lin!r}")
             opts = dict(solver_options.pop("linear_options", None) or {})
             rtol = solver_options.get("linear_rtol", 0.1)
-            amg = B200AMG(rtol=rtol, precision="mixed" if lin == "b200-mixed" else "double",
-                          **opts)
-            solver_options["linear"] = SegmentedKrylov(self.offsets, amg)
+            solver_options["linear"] = B200AMG(
+                rtol=rtol, precision="mixed" if lin == "b200-mixed" else "double",
+                segments=self.offsets, **opts)
         elif krylov != "union":
             raise ValueError(f"krylov {krylov!r}: segmented or union")
         self.solver = B200Solver(self.mesh, fluid, bcs, **solver_options)
@@ -327,5 +299,5 @@ def synthetic_ensemble(count: int = 12, low: int = 50_000, high: int = 1_200_000
     return cases
 
 
-__all__ = ["union", "segmented_fgmres", "SegmentedKrylov", "B200Ensemble", "solve_sequentially",
+__all__ = ["union", "segmented_fgmres", "B200Ensemble", "solve_sequentially",
            "vessel", "synthetic_ensemble"]
