@@ -234,7 +234,10 @@ int zvfv_bsr_spmv_t(int64_t n, const int64_t *tptr, const int32_t *trow, const i
  * Gauss-Seidel levels (AmgX's MULTICOLOR_DILU of the `dilu` presets, linear.py:571-608: the
  * diagonal E_i = A_ii - sum over earlier colours A_ij E_j^-1 A_ji, one step
  * x += omega M^-1 (b - A x) with M = (E + L) E^-1 (E + U); the transposed cycle smooths those
- * levels by transposed Gauss-Seidel); strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
+ * levels by transposed Gauss-Seidel), 4 multicolour ILU(0) on the Gauss-Seidel levels (AmgX's
+ * MULTICOLOR_ILU at sparsity level 0 of the `robust` preset: the colour-ordered level factored
+ * colour by colour without fill, one step x += omega (LU)^-1 (b - A x); transposed cycle as for
+ * DILU); strength 0 block norm (the ACM's), 1 pressure entry, 2 block norm averaged over both
  * directions of each coupling (the default of the Python back end: convection otherwise
  * stalls the pairwise matching). rebuild_every > 0 re-aggregates every that many
  * set-ups (the reference's ACM, linear.py:337-348); 0 keeps the aggregates until a solve fails

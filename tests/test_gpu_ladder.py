@@ -3,7 +3,7 @@ on the device solvers.
 
 - Driving the outer loop of a golden pipe, the ladder reaches the reference's converged fields
   (relative L2 <= 1e-8), records its probe of the robust rung at the third solve, and every
-  rung it used is one of the three device configurations.
+  rung it used is one of the four device configurations.
 - A first rung that cannot converge (its iteration budget cut to one) is abandoned for the next
   rung on the first solve, with the reason recorded, and the solve still reaches its tolerance.
 """

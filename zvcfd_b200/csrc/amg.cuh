@@ -14,7 +14,7 @@
 //  * coarse operators: Galerkin with piecewise-constant transfer, the sum of the blocks of
 //    each aggregate pair (linear.py:437-454), in a fixed order (deterministic);
 //  * smoothing: damped block Jacobi with the inverse of each 4x4 diagonal block, symmetric
-//    multicolour block Gauss-Seidel or multicolour DILU on the finest levels, or
+//    multicolour block Gauss-Seidel, DILU or ILU(0) on the finest levels, or
 //    block-Jacobi-preconditioned Chebyshev polynomials (the largest eigenvalue of D^-1 A by
 //    power iteration at set-up);
 //  * coarsest level: the explicit inverse of the dense matrix (Gauss-Jordan with partial
@@ -686,18 +686,24 @@ k_dilu_factor(long long count, long long first, const long long *__restrict__ pp
     for (int e = 0; e < 16; ++e) einv[row * 16 + e] = inv[e];
 }
 
-// One colour of the DILU solve M z = r, M = (E + L) E^-1 (E + U) (L, U: the blocks of earlier
-// and later colours), on a colour-ordered level:
+// One colour of the solve M z = r of a multicolour factorisation smoother, on a
+// colour-ordered level (L, U: the blocks of earlier and later colours).
+// DILU (ILU false): M = (E + L) E^-1 (E + U), E^-1 per row in `dinv` (row-indexed):
 //   forward (colours in order):     w_i = E_i^-1 (r_i - sum_{j earlier} A_ij w_j)
-//   backward (colours in reverse):  z_i = w_i - E_i^-1 sum_{j later} A_ij z_j,  x_i += omega z_i
-// (w and z share the vector wz). Rows split over G lanes as in the Gauss-Seidel sweep; a lane
-// loads only the blocks on its side of the colour (each pass reads half the level's blocks).
-template <int G, bool BACKWARD, typename V, typename T>
+//   backward (colours in reverse):  z_i = w_i - E_i^-1 sum_{j later} A_ij z_j
+// ILU(0) (ILU true): M = L U, `data` the factored blocks (L_ij below the colour, U_ij above,
+// U_ii^-1 at the diagonal position pdpos[i]):
+//   forward:  w_i = r_i - sum_{j earlier} L_ij w_j
+//   backward: z_i = U_ii^-1 (w_i - sum_{j later} U_ij z_j)
+// and x_i += omega z_i in the backward pass (w and z share the vector wz). Rows split over G
+// lanes as in the Gauss-Seidel sweep; a lane loads only the blocks on its side of the colour
+// (each pass reads half the level's blocks).
+template <int G, bool BACKWARD, bool ILU, typename V, typename T>
 __global__ void __launch_bounds__(256)
-k_dilu_colour(long long count, long long first, const long long *__restrict__ pptr,
-              const int *__restrict__ pidx, const V *__restrict__ data,
-              const V *__restrict__ einv, const T *__restrict__ r, T *__restrict__ wz,
-              T *__restrict__ x, T omega) {
+k_lu_colour(long long count, long long first, const long long *__restrict__ pptr,
+            const int *__restrict__ pidx, const long long *__restrict__ pdpos,
+            const V *__restrict__ data, const V *__restrict__ dinv, const T *__restrict__ r,
+            T *__restrict__ wz, T *__restrict__ x, T omega) {
     constexpr int S = G / 4;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long k = gid / G;
@@ -720,26 +726,110 @@ k_dilu_colour(long long count, long long first, const long long *__restrict__ pp
     }
 #pragma unroll
     for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    const long long i = row * 4 + rr;
     T lhs = 0;
-    if (on) lhs = BACKWARD ? acc : r[row * 4 + rr] - acc;
+    if (on) lhs = BACKWARD ? (ILU ? wz[i] - acc : acc) : r[i] - acc;
     const int base = (threadIdx.x % 32) / G * G;
     T rc[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) rc[c] = __shfl_sync(0xffffffffu, lhs, base + c);
     if (on && slot == 0) {
-        const Vec4<V> d = Vec4<V>::load(einv + row * 16 + rr * 4);
+        if (ILU && !BACKWARD) {
+            wz[i] = lhs;
+            return;
+        }
+        const V *dr = ILU ? data + pdpos[row] * 16 : dinv + row * 16;
+        const Vec4<V> d = Vec4<V>::load(dr + rr * 4);
         T s = 0;
 #pragma unroll
         for (int c = 0; c < 4; ++c) s += (T)d.v[c] * rc[c];
-        const long long i = row * 4 + rr;
         if (BACKWARD) {
-            const T z = wz[i] - s;
+            const T z = ILU ? s : wz[i] - s;
             wz[i] = z;
             x[i] += omega * z;
         } else {
             wz[i] = s;
         }
     }
+}
+
+// Multicolour ILU(0) of one colour, after the earlier colours' rows (AmgX's MULTICOLOR_ILU
+// with sparsity level 0 of the reference's `robust` preset, zvcfd/fv/linear.py:571-611): on the
+// colour-ordered level, row i (this colour) is copied from the FP64 blocks (psrc) and, for each
+// of its neighbours k of an earlier colour in increasing order, L_ik = a_ik U_kk^-1 and
+// a_ij -= L_ik U_kj for every j > k of row k that row i holds (no fill); then U_ii is inverted
+// in place. Rows of one colour are not coupled, so a colour's rows factor independently; one
+// thread per row.
+__global__ void __launch_bounds__(128)
+k_ilu_factor(long long count, long long first, const long long *__restrict__ pptr,
+             const int *__restrict__ pidx, const long long *__restrict__ psrc,
+             const long long *__restrict__ pdpos, const double *__restrict__ data,
+             double *__restrict__ lu) {
+    const long long k0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k0 >= count) return;
+    const long long row = first + k0;
+    const long long q0 = pptr[row], q1 = pptr[row + 1];
+    for (long long q = q0; q < q1; ++q)
+        for (int e = 0; e < 16; ++e) lu[q * 16 + e] = data[psrc[q] * 16 + e];
+    int prev = -1;
+    for (;;) {
+        // the next neighbour of an earlier colour, by increasing position
+        long long qk = -1;
+        int kk = (int)first;
+        for (long long q = q0; q < q1; ++q) {
+            const int j = pidx[q];
+            if (j > prev && j < kk) {
+                kk = j;
+                qk = q;
+            }
+        }
+        if (qk < 0) break;
+        prev = kk;
+        const double *Ukk = lu + pdpos[kk] * 16;       // the inverse, already in place
+        double L[16];
+        double *a = lu + qk * 16;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                double s = 0.0;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) s += a[r * 4 + m] * Ukk[m * 4 + c];
+                L[r * 4 + c] = s;
+            }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) a[e] = L[e];
+        for (long long q2 = pptr[kk]; q2 < pptr[kk + 1]; ++q2) {
+            const int j = pidx[q2];
+            if (j <= kk) continue;
+            long long q3 = -1;
+            for (long long q = q0; q < q1; ++q)
+                if (pidx[q] == j) {
+                    q3 = q;
+                    break;
+                }
+            if (q3 < 0) continue;
+            const double *Ukj = lu + q2 * 16;
+            double *aij = lu + q3 * 16;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) s += L[r * 4 + m] * Ukj[m * 4 + c];
+                    aij[r * 4 + c] -= s;
+                }
+        }
+    }
+    const long long pd = pdpos[row];
+    if (pd < 0) return;
+    double D[16], inv[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) D[e] = lu[pd * 16 + e];
+    invert4(D, inv);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) lu[pd * 16 + e] = inv[e];
 }
 
 // ------------------------------------------------------------------ multicolour Gauss-Seidel
@@ -1033,6 +1123,8 @@ struct Level {
     int *pidx = nullptr, *pinv = nullptr;                           // pinv: row -> position
     int *pagg = nullptr, *pmem = nullptr;        // aggregate of each position; members renumbered
     long long *ptrans = nullptr;                 // DILU: the position of each block's transpose
+    double *lu64 = nullptr;                      // ILU(0): the factored colour-ordered blocks
+    float *lu32 = nullptr;
     double *pdata64 = nullptr, *pdinv64 = nullptr;
     float *pdata32 = nullptr, *pdinv32 = nullptr;
     void *pb = nullptr;                          // the level's right-hand side, colour-ordered
@@ -1050,7 +1142,8 @@ struct Params {
     int precision = 0;       // 0 FP64 cycle, 1 FP32 cycle
     int smoother = 1;        // 0 damped block Jacobi, 1 symmetric multicolour block Gauss-Seidel,
                              // 2 block-Jacobi-preconditioned Chebyshev (sweeps = degree),
-                             // 3 multicolour DILU on the colour-ordered levels (Jacobi below)
+                             // 3 multicolour DILU, 4 multicolour ILU(0) on the colour-ordered
+                             // levels (Jacobi below)
     int gs_levels = 2;       // with Gauss-Seidel: the finest levels that use it (Jacobi below)
     int jacobi_sweeps = 2;   // damped block-Jacobi sweeps (pre and post) below them
     double jacobi_omega = 0.7;

@@ -845,7 +845,7 @@ class Hierarchy {
             k_diag_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.indices, nullptr, nullptr,
                                                           v.dpos); count_launch();
             k_rows_of<<<grid_for(v.n, 256), 256, 0, st>>>(v.n, v.indptr, v.rows); count_launch();
-            if ((prm.smoother == 1 || prm.smoother == 3) && v.n > DENSE_MAX && (int)l < prm.gs_levels) {
+            if ((prm.smoother == 1 || prm.smoother >= 3) && v.n > DENSE_MAX && (int)l < prm.gs_levels) {
                 if (l == 0 && coloured_indptr == v.indptr && coloured_n == v.n &&
                     coloured_nnz == v.nnz && c0.gs_rows) {
                     // the finest pattern does not change: its colouring and colour order stay
@@ -940,6 +940,10 @@ class Hierarchy {
                 ZV_TRY(values.get(&v.data32, v.nnz * 16));
                 ZV_TRY(values.get(&v.dinv32, v.n * 16));
             }
+            if (v.pptr && prm.smoother == 4) {  // ILU(0) factors (FP64, and FP32 copies)
+                ZV_TRY(values.get(&v.lu64, v.nnz * 16));
+                if (prm.precision == 1) ZV_TRY(values.get(&v.lu32, v.nnz * 16));
+            }
             if (v.pptr) {                      // the Gauss-Seidel levels' colour-ordered copy
                 if (prm.precision == 1) {
                     ZV_TRY(values.get(&v.pdata32, v.nnz * 16));
@@ -982,6 +986,7 @@ class Hierarchy {
                 }
             }
             if (v.pptr && prm.smoother == 3) ZV_TRY(dilu_factor(v));
+            if (v.pptr && prm.smoother == 4) ZV_TRY(ilu_factor(v));
             // FP32 copies in the original numbering: every level but the Gauss-Seidel ones
             // (which sweep their colour-ordered copy), and those too once A^T is solved with
             if (prm.precision == 1 && (!v.pptr || transposed_used)) ZV_TRY(convert_original(v));
@@ -1029,6 +1034,22 @@ class Hierarchy {
             scratch.release();
         }
         return launch_status("dilu factor");
+    }
+
+    // the ILU(0) factors of a colour-ordered level, colour by colour, in FP64 (converted for
+    // the FP32 hierarchy)
+    int ilu_factor(Level &v) {
+        const int C = (int)v.gs_off.size() - 1;
+        for (int c = 0; c < C; ++c) {
+            const long long o = v.gs_off[c], cnt = v.gs_off[c + 1] - o;
+            if (cnt <= 0) continue;
+            k_ilu_factor<<<grid_for(cnt, 128), 128, 0, st>>>(cnt, o, v.pptr, v.pidx, v.psrc, v.pdpos,
+                                                             v.data, v.lu64); count_launch();
+        }
+        if (prm.precision == 1) {
+            k_convert<double, float><<<grid_for(v.nnz * 16, 256), 256, 0, st>>>(v.nnz * 16, v.lu64, v.lu32); count_launch();
+        }
+        return launch_status("ilu factor");
     }
 
     int convert_original(Level &v) {
@@ -1176,17 +1197,21 @@ void gs_pass(const Level &v, const V *data, const V *dinv, const T *b, T *x, T o
     }
 }
 
-// one DILU smoothing step on a colour-ordered level: r = b - A x (b itself while x is the zero
-// start), the forward solve over the colours into w, the backward solve over them with
-// x += omega z (k_dilu_colour)
-template <typename V, typename T>
-void dilu_sweep(const Level &v, const V *data, const V *einv, const T *b, T *x, T *r, T *w, T omega,
-                bool x_zero, cudaStream_t st) {
+// one factorisation-smoother step on a colour-ordered level (DILU, or with ILU ILU(0)):
+// r = b - A x (b itself while x is the zero start), the forward solve over the colours into w,
+// the backward solve over them with x += omega z (k_lu_colour). data: the level's
+// colour-ordered blocks (A for the residual); fac: the factored blocks for ILU(0), the DILU
+// inverses E^-1 otherwise
+template <bool ILU, typename V, typename T>
+void lu_sweep(const Level &v, const V *data, const V *fac, const T *b, T *x, T *r, T *w, T omega,
+              bool x_zero, cudaStream_t st) {
     const T *rr = b;
     if (!x_zero) {
         bsr_spmv_launch<true, V, T>(v.lanes, v.n, v.pptr, v.pidx, data, x, b, r, st);
         rr = r;
     }
+    const V *blocks = ILU ? fac : data;
+    const V *dinv = ILU ? nullptr : fac;
     const int C = (int)v.gs_off.size() - 1;
     const int G = v.lanes;
     for (int back = 0; back < 2; ++back)
@@ -1195,15 +1220,19 @@ void dilu_sweep(const Level &v, const V *data, const V *einv, const T *b, T *x, 
             const long long o = v.gs_off[c], cnt = v.gs_off[c + 1] - v.gs_off[c];
             if (cnt <= 0) continue;
             const unsigned grid = grid_for(cnt * G, 256);
+#define ZV_LU_LAUNCH(GG, BB)                                                                     \
+    k_lu_colour<GG, BB, ILU, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, v.pdpos, blocks, \
+                                                          dinv, rr, w, x, omega)
             if (back) {
-                if (G == 8) k_dilu_colour<8, true, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
-                else if (G == 16) k_dilu_colour<16, true, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
-                else k_dilu_colour<32, true, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+                if (G == 8) ZV_LU_LAUNCH(8, true);
+                else if (G == 16) ZV_LU_LAUNCH(16, true);
+                else ZV_LU_LAUNCH(32, true);
             } else {
-                if (G == 8) k_dilu_colour<8, false, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
-                else if (G == 16) k_dilu_colour<16, false, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
-                else k_dilu_colour<32, false, V, T><<<grid, 256, 0, st>>>(cnt, o, v.pptr, v.pidx, data, einv, rr, w, x, omega);
+                if (G == 8) ZV_LU_LAUNCH(8, false);
+                else if (G == 16) ZV_LU_LAUNCH(16, false);
+                else ZV_LU_LAUNCH(32, false);
             }
+#undef ZV_LU_LAUNCH
             count_launch();
         }
 }
@@ -1217,6 +1246,7 @@ struct CyclePick<double> {
     static const double *inv(const Level &v) { return v.inv64; }
     static const double *pdata(const Level &v) { return v.pdata64; }
     static const double *pdinv(const Level &v) { return v.pdinv64; }
+    static const double *lu(const Level &v) { return v.lu64; }
 };
 template <>
 struct CyclePick<float> {
@@ -1225,6 +1255,7 @@ struct CyclePick<float> {
     static const float *inv(const Level &v) { return v.inv32; }
     static const float *pdata(const Level &v) { return v.pdata32; }
     static const float *pdinv(const Level &v) { return v.pdinv32; }
+    static const float *lu(const Level &v) { return v.lu32; }
 };
 
 // one V-cycle on level l: L[l].b -> L[l].x (zero initial guess); TRANS: the same cycle on
@@ -1242,7 +1273,7 @@ int Hierarchy::cycle(size_t l) {
     const auto *data = CyclePick<T>::data(v);
     const auto *dinv = CyclePick<T>::dinv(v);
     using V = typename std::remove_const<typename std::remove_pointer<decltype(data)>::type>::type;
-    const bool coloured = prm.smoother == 1 || prm.smoother == 3;
+    const bool coloured = prm.smoother == 1 || prm.smoother == 3 || prm.smoother == 4;
     const bool gs_level = coloured && !v.gs_off.empty();
     const bool jac_below = coloured && !gs_level;       // Jacobi below the GS / DILU levels
     const T omega = (T)(jac_below ? prm.jacobi_omega : prm.omega);
@@ -1260,9 +1291,14 @@ int Hierarchy::cycle(size_t l) {
         cudaMemsetAsync(px, 0, v.n * 4 * sizeof(T), st);
         bool zero = true;                 // px is still the zero start
         auto sgs = [&](int sweeps) {      // symmetric: forward then backward over the colours
-            if (prm.smoother == 3) {
-                for (int s = 0; s < sweeps; ++s, zero = false)
-                    dilu_sweep<V, T>(v, pdata, pdinv, pb, px, pr, static_cast<T *>(v.x), omega, zero, st);
+            if (prm.smoother == 3 || prm.smoother == 4) {
+                const V *lu = CyclePick<T>::lu(v);
+                for (int s = 0; s < sweeps; ++s, zero = false) {
+                    if (prm.smoother == 4)
+                        lu_sweep<true, V, T>(v, pdata, lu, pb, px, pr, static_cast<T *>(v.x), omega, zero, st);
+                    else
+                        lu_sweep<false, V, T>(v, pdata, pdinv, pb, px, pr, static_cast<T *>(v.x), omega, zero, st);
+                }
                 return;
             }
             for (int s = 0; s < sweeps; ++s) {
@@ -1850,7 +1886,7 @@ extern "C" {
 int zvfv_solver_create(void **handle, int precision, int smoother, int strength, int passes,
                        int presweeps, int postsweeps, double omega, int coarse_sweeps,
                        int max_levels, int rebuild_every, int restart) {
-    if (!handle || precision < 0 || precision > 1 || smoother < 0 || smoother > 3 || restart < 1 ||
+    if (!handle || precision < 0 || precision > 1 || smoother < 0 || smoother > 4 || restart < 1 ||
         restart > MAXV - 1 || passes < 1 || presweeps < 1 || postsweeps < 0 || max_levels < 1) {
         set_error("solver_create: bad arguments");
         return BAD_ARGUMENT;
@@ -2021,16 +2057,24 @@ int zvfv_solver_smooth(void *handle, int level, int passes, void *stream) {
                   level);
         return BAD_ARGUMENT;
     }
-    if (s->H.prm.smoother == 3) {            // DILU steps (residual, forward, backward)
+    const int sm = s->H.prm.smoother;
+    if (sm == 3 || sm == 4) {                // DILU / ILU(0) steps (residual, forward, backward)
         for (int q = 0; q < passes; ++q) {
-            if (s->H.prm.precision == 1)
-                dilu_sweep<float, float>(v, v.pdata32, v.pdinv32, static_cast<const float *>(v.pb),
-                                         static_cast<float *>(v.x2), static_cast<float *>(v.r),
-                                         static_cast<float *>(v.x), (float)s->H.prm.omega, false, st);
-            else
-                dilu_sweep<double, double>(v, v.pdata64, v.pdinv64, static_cast<const double *>(v.pb),
-                                           static_cast<double *>(v.x2), static_cast<double *>(v.r),
-                                           static_cast<double *>(v.x), s->H.prm.omega, false, st);
+            if (s->H.prm.precision == 1) {
+                const float *fac = sm == 4 ? v.lu32 : v.pdinv32;
+                float *x = static_cast<float *>(v.x2), *r = static_cast<float *>(v.r),
+                      *w = static_cast<float *>(v.x);
+                const float *b = static_cast<const float *>(v.pb);
+                if (sm == 4) lu_sweep<true, float, float>(v, v.pdata32, fac, b, x, r, w, (float)s->H.prm.omega, false, st);
+                else lu_sweep<false, float, float>(v, v.pdata32, fac, b, x, r, w, (float)s->H.prm.omega, false, st);
+            } else {
+                const double *fac = sm == 4 ? v.lu64 : v.pdinv64;
+                double *x = static_cast<double *>(v.x2), *r = static_cast<double *>(v.r),
+                       *w = static_cast<double *>(v.x);
+                const double *b = static_cast<const double *>(v.pb);
+                if (sm == 4) lu_sweep<true, double, double>(v, v.pdata64, fac, b, x, r, w, s->H.prm.omega, false, st);
+                else lu_sweep<false, double, double>(v, v.pdata64, fac, b, x, r, w, s->H.prm.omega, false, st);
+            }
         }
         return launch_status("solver_smooth");
     }
