@@ -753,7 +753,7 @@ def main():
                     help="adjoint workload: the forward solves' residual target")
     ap.add_argument("--adjoint-rtol", type=float, default=1e-10,
                     help="adjoint workload: the adjoint FGMRES tolerance")
-    ap.add_argument("--adjoint-restart", type=int, default=60,
+    ap.add_argument("--adjoint-restart", type=int, default=40,
                     help="adjoint workload: the adjoint FGMRES restart length")
     ap.add_argument("--smoother", default="gs", choices=["gs", "chebyshev", "jacobi"],
                     help="tube: the AMG smoother of both solvers")

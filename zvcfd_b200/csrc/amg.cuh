@@ -738,11 +738,15 @@ k_lu_colour(long long count, long long first, const long long *__restrict__ pptr
             wz[i] = lhs;
             return;
         }
-        const V *dr = ILU ? data + pdpos[row] * 16 : dinv + row * 16;
-        const Vec4<V> d = Vec4<V>::load(dr + rr * 4);
+        // ILU: a row without a diagonal block (none in these systems) is not smoothed
+        const long long pd = ILU ? pdpos[row] : 0;
         T s = 0;
+        if (pd >= 0) {
+            const V *dr = ILU ? data + pd * 16 : dinv + row * 16;
+            const Vec4<V> d = Vec4<V>::load(dr + rr * 4);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) s += (T)d.v[c] * rc[c];
+            for (int c = 0; c < 4; ++c) s += (T)d.v[c] * rc[c];
+        }
         if (BACKWARD) {
             const T z = ILU ? s : wz[i] - s;
             wz[i] = z;
@@ -785,6 +789,7 @@ k_ilu_factor(long long count, long long first, const long long *__restrict__ ppt
         }
         if (qk < 0) break;
         prev = kk;
+        if (pdpos[kk] < 0) continue;                    // no diagonal block: nothing to divide by
         const double *Ukk = lu + pdpos[kk] * 16;       // the inverse, already in place
         double L[16];
         double *a = lu + qk * 16;
