@@ -3,6 +3,8 @@
 - The spectral bound: ``cheb_power`` steps of the power iteration on ``D^-1 A`` of the finest
   level, restated here in NumPy from the same start vector, give the device's estimate to
   round-off.
+- On a one-level hierarchy the V-cycle is ``coarse_sweeps`` Chebyshev steps from zero,
+  restated here with the device's estimate: equal to round-off.
 - FGMRES preconditioned by the Chebyshev V-cycle solves an assembled system (FP64 and FP32
   hierarchy) and its transpose to the direct solutions.
 - The outer loop with it reaches the reference's converged fields of a golden pipe.
@@ -10,6 +12,7 @@
 
 import numpy as np
 import pytest
+import torch
 
 from fixtures import fluid_of, load, mesh_of, pipe_bcs
 from oracle.linear import bsr
@@ -77,6 +80,49 @@ def _dense_dinv_a(M, Dinv):
     for i in range(n):
         D[4 * i:4 * i + 4, 4 * i:4 * i + 4] = Dinv[i]
     return D @ M.toarray()
+
+
+def test_one_level_chebyshev_cycle_matches_restatement():
+    """One level: the V-cycle is ``coarse_sweeps`` Chebyshev steps from zero on the finest
+    level, restated here with the device's spectral estimate."""
+    import ctypes
+
+    from zvcfd_b200._lib import call
+    from zvcfd_b200.linear import B200AMG
+
+    s, A, b, x0 = _system()
+    solver = B200AMG(smoother="chebyshev", precision="double", max_levels=1, coarse_sweeps=4)
+    solver.setup(A)
+    v = ctypes.c_double()
+    call("zvfv_solver_get_option", solver._h, b"cheb_lmax", ctypes.byref(v))
+    g = torch.Generator(device="cuda").manual_seed(5)
+    r = torch.randn(A.n * 4, dtype=torch.float64, device="cuda", generator=g)
+    z = solver.vcycle(r).cpu().numpy()
+    ip, ix, data = A.indptr.cpu().numpy(), A.indices.cpu().numpy(), A.data.cpu().numpy()
+    M = bsr(ip, ix, data, A.n).tocsr()
+    blocks = data.reshape(-1, 4, 4)
+    Dinv = np.linalg.inv(np.stack([blocks[ip[i] + np.flatnonzero(ix[ip[i]:ip[i + 1]] == i)[0]]
+                                   for i in range(A.n)]))
+    hi = 1.1 * v.value
+    lo = hi / 10.0
+    theta, delta = 0.5 * (hi + lo), 0.5 * (hi - lo)
+    sigma = theta / delta
+    rh = r.cpu().numpy()
+    x = np.zeros_like(rh)
+    d = np.zeros_like(rh)
+    rho = 1.0 / sigma
+    for k in range(4):
+        zk = np.einsum("nij,nj->ni", Dinv, (rh - M @ x).reshape(-1, 4)).reshape(-1)
+        if k == 0:
+            d = zk / theta
+        else:
+            nxt = 1.0 / (2.0 * sigma - rho)
+            d = nxt * rho * d + 2.0 * nxt / delta * zk
+            rho = nxt
+        x = x + d
+    np.testing.assert_allclose(z, x, rtol=0, atol=1e-11 * np.abs(x).max())
+    solver.close()
+    s.close()
 
 
 @pytest.mark.parametrize("precision", ["double", "mixed"])
