@@ -470,10 +470,18 @@ def adjoint_workload(args):
             s.initialise(U=start[0], P=start[1])
         torch.cuda.synchronize()
         t = time.perf_counter()
-        rep = s.solve(max_iterations=3000, tol=args.adjoint_tol)
+        count = [0]
+
+        def every(msg):                      # one line in a hundred of the solve's log
+            count[0] += 1
+            if count[0] % 100 == 0:
+                log(msg)
+
+        rep = s.solve(max_iterations=3000, tol=args.adjoint_tol, log=every)
         torch.cuda.synchronize()
         return s, rep, time.perf_counter() - t
 
+    log(f"mesh: {m.n_nodes:,} nodes in {gen:.1f} s")
     s, rep, t_fwd = solve(theta0)
     log(f"forward: {rep['iterations']} outer iterations, {t_fwd:.1f} s, converged {rep['converged']}")
     res = SteadyResidual(s, z["inlet"], [z["outlet1"], z["outlet2"]], walls)
