@@ -477,7 +477,7 @@ def adjoint_workload(args):
             if count[0] % 100 == 0:
                 log(msg)
 
-        rep = s.solve(max_iterations=3000, tol=args.adjoint_tol, log=every)
+        rep = s.solve(max_iterations=args.adjoint_iterations, tol=args.adjoint_tol, log=every)
         torch.cuda.synchronize()
         return s, rep, time.perf_counter() - t
 
@@ -757,8 +757,10 @@ def main():
     ap.add_argument("--krylov", default="segmented", choices=["segmented", "union"],
                     help="ensemble: one Krylov recurrence per instance, or one over the union")
     ap.add_argument("--adjoint-nodes", type=int, default=500_000, help="adjoint workload size")
-    ap.add_argument("--adjoint-tol", type=float, default=1e-11,
+    ap.add_argument("--adjoint-tol", type=float, default=1e-10,
                     help="adjoint workload: the forward solves' residual target")
+    ap.add_argument("--adjoint-iterations", type=int, default=1000,
+                    help="adjoint workload: the forward solves' outer-iteration limit")
     ap.add_argument("--adjoint-rtol", type=float, default=1e-10,
                     help="adjoint workload: the adjoint FGMRES tolerance")
     ap.add_argument("--adjoint-restart", type=int, default=40,

@@ -518,6 +518,9 @@ k_cheby(long long n, const long long *__restrict__ ptr_, const int *__restrict__
                 for (int c = 0; c < 4; ++c) acc += (T)a.v[c] * xv.v[c];
             }
         }
+    }
+    // every lane of the warp takes part in the full-mask shuffles, rows beyond n included
+    if (!FIRST) {
 #pragma unroll
         for (int off = 4; off < G; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
     }

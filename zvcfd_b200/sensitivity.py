@@ -468,7 +468,7 @@ class SteadyResidual:
         gm = [torch.zeros((nJ,) + m.shape, dtype=m.dtype, device=m.device) if g is None else g
               for g, m in zip(gz[2:], mz)]
         lam, its, res = self.adjoint_batched(gx, gm, x, mdot, theta, rtol=rtol,
-                                             restart=min(restart, 60), maxiter=maxiter)
+                                             restart=restart, maxiter=maxiter)
         th2 = theta.detach().requires_grad_(True)
         r, gmd, _ = self.residual(x, mdot, th2)
         dR = torch.autograd.grad([r] + gmd, th2, [lam[0].reshape(nJ, *r.shape)] +
@@ -743,11 +743,14 @@ class TransientSensitivity:
 
 
 def fgmres_batched(A, b, M, *, rtol=1e-10, restart=40, maxiter=400):
-    """B right-preconditioned FGMRES recurrences in lock-step: ``b (B, n)``, ``A`` and ``M``
-    map ``(B, n)`` to ``(B, n)`` row by row. Classical Gram-Schmidt applied twice (one batched
-    product per pass over a preallocated basis), Givens rotations per system on the host; a
-    system that reaches ``rtol`` (relative to ``|b|``) or breaks down freezes (its later basis
-    vectors are zero) while the others go on. Returns ``(x, steps, residuals (B,))``."""
+    """B right-preconditioned GMRES recurrences in lock-step: ``b (B, n)``, ``A`` and ``M``
+    map ``(B, n)`` to ``(B, n)`` row by row, ``M`` a fixed linear operator (the transposed
+    V-cycle is one: fixed sweeps, no inner tolerance), so that only the basis is stored and
+    each restart cycle's update is ``M`` applied once to its combination of basis vectors (half
+    the memory of the flexible form). Classical Gram-Schmidt applied twice (one batched product
+    per pass over a preallocated basis), Givens rotations per system on the host; a system that
+    reaches ``rtol`` (relative to ``|b|``) or breaks down freezes (its later basis vectors are
+    zero) while the others go on. Returns ``(x, steps, residuals (B,))``."""
     B, n = b.shape
     dt, dev = b.dtype, b.device
     x = torch.zeros_like(b)
@@ -755,7 +758,6 @@ def fgmres_batched(A, b, M, *, rtol=1e-10, restart=40, maxiter=400):
     bn_safe = np.where(bn > 0, bn, 1.0)
     m = restart
     Vb = torch.zeros((m + 1, B, n), dtype=dt, device=dev)
-    Zb = torch.zeros((m, B, n), dtype=dt, device=dev)
     r = b.clone()
     it = 0
     res = np.zeros(B)
@@ -774,8 +776,7 @@ def fgmres_batched(A, b, M, *, rtol=1e-10, restart=40, maxiter=400):
         steps = np.where(live, -1, 0)                       # -1 while a system is active
         k_used = 0
         for k in range(m):
-            Zb[k] = M(Vb[k])
-            w = A(Zb[k])
+            w = A(M(Vb[k]))
             V = Vb[:k + 1]
             h = np.zeros((B, k + 1))
             for _ in range(2):
@@ -811,7 +812,8 @@ def fgmres_batched(A, b, M, *, rtol=1e-10, restart=40, maxiter=400):
             K = k_used if steps[q] < 0 else steps[q]
             if K:
                 Y[q, :K] = np.linalg.solve(np.triu(H[q, :K, :K]), g[q, :K])
-        x = x + torch.einsum("bj,jbn->bn", torch.as_tensor(Y, dtype=dt, device=dev), Zb[:k_used])
+        x = x + M(torch.einsum("bj,jbn->bn", torch.as_tensor(Y, dtype=dt, device=dev),
+                               Vb[:k_used]))
         r = b - A(x)
     return x, it, res
 
