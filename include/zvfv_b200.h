@@ -272,11 +272,14 @@ int zvfv_solver_solve_t(void *handle, const double *b, double *x, double rtol, i
  * from 0 to n. The operator and the V-cycle act on all segments at once; inner products, norms,
  * Hessenberg columns, rotations and step lengths are per segment, and each segment stops at
  * rtol times its own initial residual (floor 1e-13 of its right-hand side's norm). The solve
- * ends when all have, or after maxiter Krylov steps (shared). residuals, converged: n_segments
- * host values. No reference counterpart (the reference solves one problem per solver).
- * Other arguments as zvfv_solver_solve. */
+ * ends when all have, or after maxiter Krylov steps (shared). active: n_segments host flags,
+ * or null for all; a segment marked 0 takes no steps and keeps its initial guess (an instance
+ * that has already converged). residuals, converged: n_segments host values. No reference
+ * counterpart (the reference solves one problem per solver). Other arguments as
+ * zvfv_solver_solve. */
 int zvfv_solver_solve_segmented(void *handle, int n_segments, const int64_t *row_bounds,
-                                const double *b, double *x, double rtol, int maxiter,
+                                const int *active, const double *b, double *x, double rtol,
+                                int maxiter,
                                 int n_lowrank, const int64_t *const *u_idx,
                                 const double *const *u_val, const int64_t *u_len,
                                 const int64_t *const *w_idx, const double *const *w_val,

@@ -5,7 +5,8 @@ hexahedral/prismatic tube) form one block-diagonal system, the second block's ri
 scaled down by 1e-6 so that a single recurrence over the union would leave it unreduced. The
 segmented solve must bring each block to 1e-10 of its own initial residual and to its own
 direct solution, in FP64 and with the FP32 hierarchy, and report each block's residual; a
-block with nothing to solve (zero right-hand side and guess) takes no steps and stays zero.
+block with nothing to solve (zero right-hand side and guess) takes no steps and stays zero, and
+a block marked inactive keeps its initial guess.
 """
 
 import numpy as np
@@ -80,5 +81,15 @@ def test_segmented_fgmres_reaches_every_block_on_its_own(precision):
     assert ok2.all() and res2[1] == 0.0, res2
     assert not bool(x2[4 * bounds[1]:].any())
     np.testing.assert_allclose(x2[:4 * bounds[1]].cpu().numpy(), xh[:4 * bounds[1]],
+                               atol=1e-8 * np.abs(xh[:4 * bounds[1]]).max())
+    # a block marked inactive keeps its initial guess exactly while the other is solved
+    guess = torch.cat([torch.zeros(4 * bounds[1], dtype=torch.float64, device="cuda"),
+                       torch.ones(4 * (bounds[2] - bounds[1]), dtype=torch.float64, device="cuda")])
+    solver.segment_active = [True, False]
+    x3, info3 = solver.solve(A, b, guess)
+    solver.segment_active = None
+    assert info3.converged, info3
+    assert torch.equal(x3[4 * bounds[1]:], guess[4 * bounds[1]:])
+    np.testing.assert_allclose(x3[:4 * bounds[1]].cpu().numpy(), xh[:4 * bounds[1]],
                                atol=1e-8 * np.abs(xh[:4 * bounds[1]]).max())
     solver.close()

@@ -63,8 +63,8 @@ _SIGNATURES = {
     "zvfv_solver_setup": ([P, I64, I64, P, P, P, P], None),
     "zvfv_solver_solve": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
     "zvfv_solver_solve_t": ([P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P, P], None),
-    "zvfv_solver_solve_segmented": ([P, I32, P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P, P,
-                                     P], None),
+    "zvfv_solver_solve_segmented": ([P, I32, P, P, P, P, F64, I32, I32, P, P, P, P, P, P, P, P,
+                                     P, P], None),
     "zvfv_solver_vcycle": ([P, P, P, P], None),
     "zvfv_solver_set_option": ([P, ctypes.c_char_p, F64], None),
     "zvfv_solver_get_option": ([P, ctypes.c_char_p, P], None),

@@ -292,14 +292,16 @@ __global__ void k_seg_fold(const int *__restrict__ sfirst, int cols, const doubl
 
 // per segment at the start of a solve: beta0 = |r|, target = max(rtol beta0, 1e-13 |b|)
 // (the floor of the single-recurrence solve); bb, rr: folded squares (MAXV-strided)
+// A segment marked inactive (active[s] == 0) gets an infinite target: it takes no steps and
+// keeps its initial guess.
 __global__ void k_seg_targets(int nseg, double rtol, const double *__restrict__ bb,
-                              const double *__restrict__ rr, double *__restrict__ beta0,
-                              double *__restrict__ target) {
+                              const double *__restrict__ rr, const int *__restrict__ active,
+                              double *__restrict__ beta0, double *__restrict__ target) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nseg) return;
     const double b0 = sqrt(rr[(long long)s * MAXV]);
     beta0[s] = b0;
-    target[s] = fmax(rtol * b0, 1e-13 * sqrt(bb[(long long)s * MAXV]));
+    target[s] = active[s] ? fmax(rtol * b0, 1e-13 * sqrt(bb[(long long)s * MAXV])) : INFINITY;
 }
 
 // a restart cycle's first column: g = (beta, 0, ...), the segment active (kk = -1) while its
@@ -1677,7 +1679,7 @@ struct Solver {
     int nseg = 0, nsc = 0;                 // segments, CTAs of a segmented pass
     long long seg_n4 = 0;
     long long *cfirst = nullptr;
-    int *cseg = nullptr, *sfirst = nullptr, *kk = nullptr, *cnt = nullptr;
+    int *cseg = nullptr, *sfirst = nullptr, *kk = nullptr, *cnt = nullptr, *sact = nullptr;
     double *spart = nullptr, *sh1 = nullptr, *sh2 = nullptr, *snrm = nullptr, *sbb = nullptr;
     double *srr = nullptr, *sbeta0 = nullptr, *starget = nullptr, *sH = nullptr, *scs = nullptr;
     double *ssn = nullptr, *sg = nullptr, *sy = nullptr, *sst = nullptr, *sinv = nullptr;
@@ -1719,6 +1721,7 @@ struct Solver {
         ZV_TRY(segwork.get(&cseg, std::max(nsc, 1)));
         ZV_TRY(segwork.get(&sfirst, ns + 1));
         ZV_TRY(segwork.get(&kk, ns));
+        ZV_TRY(segwork.get(&sact, ns));
         ZV_TRY(segwork.get(&cnt, 1));
         ZV_TRY(segwork.get(&spart, (size_t)std::max(nsc, 1) * MAXV));
         for (double **q : {&sh1, &sh2, &snrm, &sbb, &srr, &sy}) ZV_TRY(segwork.get(q, (size_t)ns * MAXV));
@@ -1755,10 +1758,18 @@ struct Solver {
         return OK;
     }
 
-    int solve_segmented(int ns, const long long *rows, const double *b, double *xio, double rtol,
-                        int maxiter, const std::vector<LowRank> &lr, int *iterations,
-                        double *residuals, int *converged) {
+    int solve_segmented(int ns, const long long *rows, const int *active, const double *b,
+                        double *xio, double rtol, int maxiter, const std::vector<LowRank> &lr,
+                        int *iterations, double *residuals, int *converged) {
         ZV_TRY(ensure_segments(ns, rows));
+        {
+            std::vector<int> on(ns, 1);
+            if (active)
+                for (int q = 0; q < ns; ++q) on[q] = active[q] ? 1 : 0;
+            ZV_TRY(cuda_status(cudaMemcpyAsync(sact, on.data(), ns * sizeof(int),
+                                               cudaMemcpyHostToDevice, st), "segments: active"));
+            ZV_TRY(cuda_status(cudaStreamSynchronize(st), "segments: active"));
+        }
         if (nsc == 0) {
             *iterations = 0;
             for (int q = 0; q < ns; ++q) {
@@ -1773,7 +1784,7 @@ struct Solver {
         ZV_TRY(apply(x, b, r, lr));
         seg_norm2(b, sbb);
         seg_norm2(r, srr);
-        k_seg_targets<<<gs, 128, 0, st>>>(ns, rtol, sbb, srr, sbeta0, starget); count_launch();
+        k_seg_targets<<<gs, 128, 0, st>>>(ns, rtol, sbb, srr, sact, sbeta0, starget); count_launch();
         int it = 0, open = 0;
         while (it < maxiter) {
             cudaMemsetAsync(cnt, 0, sizeof(int), st);
@@ -1948,9 +1959,11 @@ int zvfv_solver_solve(void *handle, const double *b, double *x, double rtol, int
 // ascending host values from 0 to n): the block-diagonal system of independent instances.
 // Each segment stops at its own target, rtol times its initial residual (floor 1e-13 |b_s|);
 // the solve ends when every segment has, or after maxiter Krylov steps (shared by all).
+// active: n_segments host flags or null; a segment marked 0 takes no steps and keeps its guess.
 // residuals / converged: n_segments host values (relative residual, 0/1).
 int zvfv_solver_solve_segmented(void *handle, int n_segments, const int64_t *row_bounds,
-                                const double *b, double *x, double rtol, int maxiter,
+                                const int *active, const double *b, double *x, double rtol,
+                                int maxiter,
                                 int n_lowrank, const int64_t *const *u_idx,
                                 const double *const *u_val, const int64_t *u_len,
                                 const int64_t *const *w_idx, const double *const *w_val,
@@ -1968,8 +1981,8 @@ int zvfv_solver_solve_segmented(void *handle, int n_segments, const int64_t *row
     for (int q = 0; q < n_lowrank; ++q)
         lr.push_back({(const long long *)u_idx[q], u_val[q], (long long)u_len[q],
                       (const long long *)w_idx[q], w_val[q], (long long)w_len[q]});
-    return s->solve_segmented(n_segments, (const long long *)row_bounds, b, x, rtol, maxiter, lr,
-                              iterations, residuals, converged);
+    return s->solve_segmented(n_segments, (const long long *)row_bounds, active, b, x, rtol,
+                              maxiter, lr, iterations, residuals, converged);
 }
 
 // the adjoint solve: A^T x = b with the same hierarchy, transposed (same arguments)

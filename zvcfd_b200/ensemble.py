@@ -183,8 +183,11 @@ class B200Ensemble:
         done = np.zeros(self.n, bool)
         first = np.full(self.n, -1)
         hist = []
+        seg = getattr(s.linear, "segments", None) is not None
         for it in range(max_iterations):
             U0, P0 = s.U.clone(), s.P.clone()
+            if seg:                 # converged instances stop: their blocks keep the state
+                s.linear.segment_active = ~done
             rec = s.iterate()
             du = self._per_instance((s.U - U0).abs().amax(1), "max")
             um = self._per_instance(s.U.abs().amax(1), "max")
