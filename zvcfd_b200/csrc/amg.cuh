@@ -1114,6 +1114,7 @@ struct Level {
     double *dinv64 = nullptr;
     float *data32 = nullptr, *dinv32 = nullptr;
     int lanes = 8;
+    int gs_depth = 1;                     // Gauss-Seidel blocks in flight: 0 half, 1 base, 2 double
     // transfer to the next level (kept while the aggregation is kept)
     int *agg = nullptr;
     long long nc = 0;

@@ -1171,6 +1171,19 @@ void launch_dependent(void (*kern)(P...), unsigned grid, cudaStream_t st, A... a
     cudaLaunchKernelEx(&cfg, kern, static_cast<P>(args)...);
 }
 
+// one colour of a Gauss-Seidel pass with B blocks per slot in flight (the base for G lanes), or
+// half (sel 0) or twice (sel 2) that many, capped at 16: the level's tile shape, which the
+// autotuner picks with the lanes per row
+template <int G, int B, typename V, typename T>
+void gs_colour_launch(int sel, unsigned grid, cudaStream_t st, long long cnt, long long o, const Level &v,
+                      const V *data, const V *dinv, const T *b, T *x, T omega) {
+    constexpr int LO = B / 2 > 0 ? B / 2 : 1;
+    constexpr int HI = 2 * B < 16 ? 2 * B : 16;
+    if (sel == 0) launch_dependent(k_gs_colour_pdl<G, LO, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
+    else if (sel == 2) launch_dependent(k_gs_colour_pdl<G, HI, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
+    else launch_dependent(k_gs_colour_pdl<G, B, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
+}
+
 // one Gauss-Seidel pass over the colours of level v, forward or backward: on the colour-ordered
 // copy (data, dinv, b, x colour-ordered; each colour a contiguous row range), or with TRANS on
 // A^T in the original numbering (columns of A through the transpose structure, D^-T)
@@ -1191,9 +1204,9 @@ void gs_pass(const Level &v, const V *data, const V *dinv, const T *b, T *x, T o
             else k_gs_colour_t<32, V, T><<<grid, 256, 0, st>>>(cnt, rows, v.tptr, v.trow, v.tperm, data, dinv, b, x, omega);
         } else {
             constexpr int D = gs_prefetch_depth<V>();
-            if (G == 8) launch_dependent(k_gs_colour_pdl<8, 2 * D, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
-            else if (G == 16) launch_dependent(k_gs_colour_pdl<16, D, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
-            else launch_dependent(k_gs_colour_pdl<32, (D + 1) / 2, V, T>, grid, st, cnt, o, v.pptr, v.pidx, data, dinv, b, x, omega);
+            if (G == 8) gs_colour_launch<8, 2 * D, V, T>(v.gs_depth, grid, st, cnt, o, v, data, dinv, b, x, omega);
+            else if (G == 16) gs_colour_launch<16, D, V, T>(v.gs_depth, grid, st, cnt, o, v, data, dinv, b, x, omega);
+            else gs_colour_launch<32, (D + 1) / 2, V, T>(v.gs_depth, grid, st, cnt, o, v, data, dinv, b, x, omega);
         }
         count_launch();
     }
@@ -1426,11 +1439,11 @@ int Hierarchy::cycle(size_t l) {
     return launch_status("v-cycle");
 }
 
-// The lanes-per-row autotuner: after each rebuild, every level of at least AUTOTUNE_MIN_ROWS
-// rows times one smoothing pass (a forward Gauss-Seidel pass over its colours, or a Jacobi
-// sweep) with 8, 16 and 32 lanes per row, twice each after a warm-up, with CUDA events on the
-// solver's stream, and keeps the fastest for all of that level's row kernels (smoothing,
-// residual). Different lanes add a row's blocks in a different order, so with the autotuner
+// The autotuner: after each rebuild, every level of at least AUTOTUNE_MIN_ROWS rows times one
+// smoothing pass (a forward Gauss-Seidel pass over its colours, or a Jacobi sweep) with 8, 16
+// and 32 lanes per row and, on a Gauss-Seidel level, with half, the base and twice the blocks
+// in flight per slot, twice each after a warm-up, with CUDA events on the solver's stream, and
+// keeps the fastest for all of that level's row kernels (smoothing, residual). Different lanes add a row's blocks in a different order, so with the autotuner
 // on, two runs can differ in the last bits when their timings pick differently.
 constexpr long long AUTOTUNE_MIN_ROWS = 2048;
 
@@ -1450,27 +1463,31 @@ int Hierarchy::autotune() {
         T *b = static_cast<T *>(gs ? v.pb : v.b), *x = static_cast<T *>(v.x2), *y = static_cast<T *>(v.x);
         cudaMemsetAsync(b, 0, v.n * 4 * sizeof(T), st);
         cudaMemsetAsync(x, 0, v.n * 4 * sizeof(T), st);
-        int best = v.lanes;
+        int best = v.lanes, best_depth = v.gs_depth;
         float best_ms = 1e30f;
-        for (int G : {8, 16, 32}) {
-            v.lanes = G;
-            float total = 0.0f;
-            for (int rep = 0; rep < 3 && rc == OK; ++rep) {
-                cudaEventRecord(e0, st);
-                if (gs) gs_pass<false, V, T>(v, data, dinv, b, x, (T)0.5, false, st);
-                else jacobi<false>(G, v.n, v.indptr, v.indices, data, dinv, b, x, y, (T)0.5, st);
-                cudaEventRecord(e1, st);
-                rc = cuda_status(cudaEventSynchronize(e1), "autotune");
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (rep > 0) total += ms;
+        for (int G : {8, 16, 32})
+            for (int sel = 0; sel < (gs ? 3 : 1); ++sel) {    // Gauss-Seidel: blocks in flight too
+                v.lanes = G;
+                v.gs_depth = gs ? sel : 1;
+                float total = 0.0f;
+                for (int rep = 0; rep < 3 && rc == OK; ++rep) {
+                    cudaEventRecord(e0, st);
+                    if (gs) gs_pass<false, V, T>(v, data, dinv, b, x, (T)0.5, false, st);
+                    else jacobi<false>(G, v.n, v.indptr, v.indices, data, dinv, b, x, y, (T)0.5, st);
+                    cudaEventRecord(e1, st);
+                    rc = cuda_status(cudaEventSynchronize(e1), "autotune");
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (rep > 0) total += ms;
+                }
+                if (total < best_ms) {
+                    best_ms = total;
+                    best = G;
+                    best_depth = v.gs_depth;
+                }
             }
-            if (total < best_ms) {
-                best_ms = total;
-                best = G;
-            }
-        }
         v.lanes = best;
+        v.gs_depth = best_depth;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
