@@ -13,11 +13,11 @@ is larger than L2, so no flush is needed between steps.
 
 ``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]``
 
-Three further workloads print their own line (``--workload bifurcation``: the ~2M-node
+Four further workloads print their own lines (``--workload bifurcation``: the ~2M-node
 transient Y-bifurcation, mixed vs FP64 per BDF2 step; ``--workload ensemble``: 12 vessels
 solved together vs one after another; ``--workload adjoint``: the adjoint gradient of the
-~500k-node steady Y-bifurcation, checked against central differences); the default is the
-headline above. ``--smoother chebyshev`` runs the headline with the Chebyshev smoother.
+~500k-node steady Y-bifurcation, checked against central differences; ``--workload smoothers``:
+the AMG smoothers compared on the headline tube); the default is the headline above. ``--smoother chebyshev`` runs the headline with the Chebyshev smoother.
 """
 
 from __future__ import annotations
@@ -421,6 +421,61 @@ def ensemble_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def smoothers_workload(args):
+    """The AMG smoothers compared on the headline tube: per configuration (precision,
+    smoother, degree or sweeps), the mean outer-iteration time and Krylov steps of iterations
+    4-11, one V-cycle and one finest-level smoothing pass (CUDA events), the spectral estimate
+    of the Chebyshev smoother, and the steady solve to 1e-8 from scratch. One JSON line per
+    configuration."""
+    import ctypes
+
+    import torch
+
+    from zvcfd_b200._lib import call, stream_ptr
+    from zvcfd_b200.solver import B200Solver
+
+    m, fl, bcs = make_case(args.axial)
+    cheb = {"smoother": "chebyshev", "presweeps": 2, "postsweeps": 2}
+    runs = [("b200", {"smoother": "gs"}), ("b200", cheb),
+            ("b200", {"smoother": "chebyshev", "presweeps": 3, "postsweeps": 3}),
+            ("b200", {"smoother": "dilu"}), ("b200", {"smoother": "ilu0"}),
+            ("b200-mixed", {"smoother": "gs"}), ("b200-mixed", cheb),
+            ("b200-mixed", {"smoother": "dilu"})]
+    for lin, opts in runs:
+        s = B200Solver(m, fl, bcs, linear=lin, linear_rtol=0.1, linear_options=opts)
+        for _ in range(3):
+            s.iterate()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        its = [s.iterate()["linear_iterations"] for _ in range(8)]
+        torch.cuda.synchronize()
+        per = (time.perf_counter() - t) / 8
+        A, b, _, x0 = s._assemble_fused()
+        s.linear.setup(A)
+        r = b.reshape(-1) - A.matvec(x0)
+        tv = event_time(lambda: s.linear.vcycle(r), reps=10)
+        tp = event_time(lambda: call("zvfv_solver_smooth", s.linear._h, 0, 1, stream_ptr()),
+                        reps=10)
+        lmax = None
+        if opts["smoother"] == "chebyshev":
+            v = ctypes.c_double()
+            call("zvfv_solver_get_option", s.linear._h, b"cheb_lmax", ctypes.byref(v))
+            lmax = v.value
+        s.close()
+        s2 = B200Solver(m, fl, bcs, linear=lin, linear_rtol=0.1, linear_options=opts)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rep = s2.solve(max_iterations=80, tol=1e-8)
+        torch.cuda.synchronize()
+        s2.close()
+        print(json.dumps({"workload": WORKLOAD, "linear": lin, **opts,
+                          "ms_per_outer_iteration": per * 1e3, "krylov_steps": its,
+                          "vcycle_ms": tv * 1e3, "finest_pass_ms": tp * 1e3,
+                          "cheb_lmax": lmax, "to_1e-8_s": time.perf_counter() - t0,
+                          "outer_iterations": rep["iterations"],
+                          "converged": rep["converged"]}), flush=True)
+
+
 def adjoint_workload(args):
     """The adjoint workload: the Y-bifurcation coarsened to about 500k nodes, steady,
     Carreau-Yasuda blood, a 1 ml/s inlet and RCR outlets (Rp 1e8, C 1e-9, Rd 1e9), a fixed
@@ -745,9 +800,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stages", action="store_true")
     ap.add_argument("--workload", default="tube",
-                    choices=["tube", "bifurcation", "ensemble", "adjoint"],
+                    choices=["tube", "bifurcation", "ensemble", "adjoint", "smoothers"],
                     help="tube: the headline (default); bifurcation: the 2M-node transient; "
-                         "ensemble: the 12-vessel batch; adjoint: the 500k-node steady gradient")
+                         "ensemble: the 12-vessel batch; adjoint: the 500k-node steady "
+                         "gradient; smoothers: the AMG smoothers compared on the headline tube")
     ap.add_argument("--nodes", type=int, default=2_000_000, help="bifurcation workload size")
     ap.add_argument("--loops", type=int, default=5,
                     help="bifurcation: coefficient loops per time step at most (the reference's 5)")
@@ -782,7 +838,7 @@ def main():
         torch.cuda.set_device(local)
         if rank == 0:
             {"bifurcation": bifurcation_workload, "ensemble": ensemble_workload,
-             "adjoint": adjoint_workload}[args.workload](args)
+             "adjoint": adjoint_workload, "smoothers": smoothers_workload}[args.workload](args)
         return
 
     import torch
