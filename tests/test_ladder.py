@@ -116,3 +116,26 @@ def test_the_device_ladder_is_named_like_the_reference():
     with pytest.raises(ValueError, match="b200-auto"):
         linear.make("amgx")
     assert Ladder.name == "auto"
+
+
+def test_presets_restate_the_reference_amgx_presets():
+    """``B200AMG(preset=...)`` takes the reference's AmgX preset names and sets the smoother,
+    sweeps and relaxation of each; explicit arguments win."""
+    from zvcfd_b200.linear import PRESETS, B200AMG
+
+    assert set(PRESETS) == {"gs", "robust", "dilu-p", "dilu"}
+    want = {"gs": ("gs", 1, 2), "robust": ("ilu0", 1, 1), "dilu-p": ("dilu", 1, 2),
+            "dilu": ("dilu", 1, 2)}
+    for name, (smoother, pre, post) in want.items():
+        a = B200AMG(preset=name)
+        assert (a.smoother, a.presweeps, a.postsweeps) == (smoother, pre, post), name
+        a.close()
+    a = B200AMG(preset="robust", smoother="gs")
+    assert a.smoother == "gs"
+    a.close()
+    try:
+        B200AMG(preset="nope")
+    except ValueError as e:
+        assert "preset" in str(e)
+    else:
+        raise AssertionError("an unknown preset is accepted")
