@@ -821,8 +821,9 @@ def main():
                     help="adjoint workload: the adjoint FGMRES tolerance")
     ap.add_argument("--adjoint-restart", type=int, default=40,
                     help="adjoint workload: the adjoint FGMRES restart length")
-    ap.add_argument("--smoother", default="gs", choices=["gs", "chebyshev", "jacobi"],
-                    help="tube: the AMG smoother of both solvers")
+    ap.add_argument("--smoother", default=None,
+                    choices=["chebyshev", "gs", "dilu", "ilu0", "jacobi"],
+                    help="tube: the AMG smoother of both solvers (default: the library's)")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark the timed steps with an NVTX range 'timed' (for ncu --nvtx-include)")
     args = ap.parse_args()
@@ -857,7 +858,7 @@ def main():
     m, fl, bcs = make_case(args.axial)
     # two identical solvers: `value` is timed on one, `e2e` on the other over the same outer
     # iterations (warm-up + 1 .. warm-up + steps) - the device work is deterministic
-    lopts = {"smoother": args.smoother}
+    lopts = {} if args.smoother is None else {"smoother": args.smoother}
     solver = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1, linear_options=lopts)
     twin = B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1, linear_options=lopts)
     for _ in range(args.warmup):
@@ -927,10 +928,10 @@ def main():
                      "fp64_frac": sp["fp64"]["gbs"] / peak, "nnzb": nnzb, "rows": n}
     roof = None
     if not args.no_stages:
-        stages, hstats = stage_times(solver, peak, smoother=args.smoother)
-        mstages, _ = stage_times(mixed, peak, 4, smoother=args.smoother)
+        stages, hstats = stage_times(solver, peak, smoother=solver.linear.smoother)
+        mstages, _ = stage_times(mixed, peak, 4, smoother=mixed.linear.smoother)
         ib = iteration_bytes(solver, hstats, extra["fp64_linear_iterations"],
-                             smoother=args.smoother)
+                             smoother=solver.linear.smoother)
         extra["stages"] = {"fp64": stages,
                            "mixed": {k: mstages[k] for k in ("vcycle", "gs_pass")}}
         extra["outer_iteration_roofline"] = {
@@ -945,8 +946,9 @@ def main():
                 "peak": peak, "unit": "GB/s", "frac": g["frac"], "peak_source": peak_source,
                 "algorithmic_bytes": g["algorithmic_bytes"],
                 "traffic": None if GS_TRAFFIC_PER_ALGORITHMIC_BYTE is None or
-                args.smoother != "gs" else GS_TRAFFIC_PER_ALGORITHMIC_BYTE * g["algorithmic_bytes"],
-                "traffic_source": GS_TRAFFIC_SOURCE if args.smoother == "gs" else None}
+                solver.linear.smoother != "gs"
+                else GS_TRAFFIC_PER_ALGORITHMIC_BYTE * g["algorithmic_bytes"],
+                "traffic_source": GS_TRAFFIC_SOURCE if solver.linear.smoother == "gs" else None}
     if not args.no_converge and rank == 0:
         conv = {}
         for tag, lin in (("fp64", "b200"), ("mixed", "b200-mixed")):
@@ -988,7 +990,7 @@ def main():
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "nodes": N, "blocks": nnzb,
                            "precision": "fp64 (mixed below)", "linear_rtol": 0.1,
-                           "smoother": args.smoother,
+                           "smoother": solver.linear.smoother,
                            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32 * N,
                         "d2h_bytes_per_step": 32 * N + 8 * 29},

@@ -93,8 +93,9 @@ def test_one_level_chebyshev_cycle_matches_restatement():
     s, A, b, x0 = _system()
     solver = B200AMG(smoother="chebyshev", precision="double", max_levels=1, coarse_sweeps=4)
     solver.setup(A)
-    v = ctypes.c_double()
+    v, ratio = ctypes.c_double(), ctypes.c_double()
     call("zvfv_solver_get_option", solver._h, b"cheb_lmax", ctypes.byref(v))
+    call("zvfv_solver_get_option", solver._h, b"cheb_ratio", ctypes.byref(ratio))
     g = torch.Generator(device="cuda").manual_seed(5)
     r = torch.randn(A.n * 4, dtype=torch.float64, device="cuda", generator=g)
     z = solver.vcycle(r).cpu().numpy()
@@ -104,7 +105,7 @@ def test_one_level_chebyshev_cycle_matches_restatement():
     Dinv = np.linalg.inv(np.stack([blocks[ip[i] + np.flatnonzero(ix[ip[i]:ip[i + 1]] == i)[0]]
                                    for i in range(A.n)]))
     hi = 1.1 * v.value
-    lo = hi / 10.0
+    lo = hi / ratio.value
     theta, delta = 0.5 * (hi + lo), 0.5 * (hi - lo)
     sigma = theta / delta
     rh = r.cpu().numpy()

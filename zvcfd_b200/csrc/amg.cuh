@@ -1165,7 +1165,7 @@ struct Params {
     int rebuild_every = 0;   // > 0: re-aggregate every this many set-ups; 0: adaptively
     double rebuild_ratio = 1.5;   // adaptive: rebuild after a solve needing more iterations
     int autotune = 0;        // 1: time each level's smoother at 8, 16 and 32 lanes per row
-    double cheb_ratio = 10.0;   // Chebyshev: the interval [hi / ratio, hi], hi = 1.1 lambda_max
+    double cheb_ratio = 4.0;    // Chebyshev: the interval [hi / ratio, hi], hi = 1.1 lambda_max
     int cheb_power = 10;        // power-iteration steps estimating lambda_max of D^-1 A
 };
 
