@@ -18,7 +18,8 @@ methods of two converged cases (``forces``); WSS time statistics (``wss``);
 the manufactured Carreau-Yasuda outlet (``gn_outlet``); developed inlet
 profiles and a pipe with the default flow-rate inlet (``profiles``); uneven BDF2 steps of
 an oscillating pipe (``variable_steps``); a mid-size curved Carreau-Yasuda tube
-(``curved_mid``, about 6k nodes, the bench tube's cross-section coarsened). A single file is
+(``curved_mid``, about 6k nodes, the bench tube's cross-section coarsened); Morton owners,
+local meshes and halo plans of the reference's partitioner (``partition``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -531,7 +532,50 @@ def lumped_case() -> dict:
     return out
 
 
+def partition_case() -> dict:
+    """The reference's partitions (``zvcfd/fv/partition.py``) of the meshes of its own
+    partition test (``tests/test_fv_multi.py:40-43``: a mixed tube, 4 parts) and of the golden
+    pipe (2, 3 and 4 parts, and 3 parts at a given chunk edge): owners, and per part the local
+    nodes, owned count, held elements and faces and the halo plan, flattened."""
+    from zvcfd.fv.partition import halo_plan, local_meshes, morton_owner
+
+    out = {}
+    tubes = {"mixed": tube(0.5, 2.0, n_core=3, n_ring=3, n_axial=16, kind="mixed", layers=1),
+             "pipe": tube(0.5, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed", layers=1)}
+    runs = [("mixed", 4, None), ("pipe", 2, None), ("pipe", 3, None), ("pipe", 4, None),
+            ("pipe", 3, 0.3)]
+    for name, m in tubes.items():
+        for k, v in mesh_arrays(m).items():
+            out[f"{name}_{k}"] = v
+    for i, (name, n, chunk) in enumerate(runs):
+        m = tubes[name]
+        owner = morton_owner(m.nodes, n, chunk)
+        parts = local_meshes(m, owner)
+        plans = halo_plan(parts, owner)
+        tag = f"run{i}"
+        out[f"{tag}_meta"] = np.array([n, -1.0 if chunk is None else chunk])
+        out[f"{tag}_mesh"] = np.array(name)
+        out[f"{tag}_owner"] = owner
+        for p, (lm, plan) in enumerate(zip(parts, plans)):
+            out[f"{tag}_p{p}_nodes"] = lm.nodes
+            out[f"{tag}_p{p}_n_own"] = np.array(lm.n_own)
+            for k, sel in lm.elements.items():
+                out[f"{tag}_p{p}_elem_{k}"] = sel
+            for z, sel in lm.faces.items():
+                out[f"{tag}_p{p}_face_{z}"] = sel
+            out[f"{tag}_p{p}_plan"] = np.array([q for q, _, _ in plan], np.int64)
+            for q, send, recv in plan:
+                out[f"{tag}_p{p}_send_{q}"] = send
+                out[f"{tag}_p{p}_recv_{q}"] = recv
+    out["runs"] = np.array(len(runs))
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["partition"]:
+        np.savez_compressed(HERE / "partition.npz", **partition_case())
+        print("wrote partition")
+        return
     if sys.argv[1:] == ["kernels"]:
         for name in MESHES:
             for gn, dt in VARIANTS:
@@ -611,6 +655,8 @@ def main():
     print("wrote profiles")
     np.savez_compressed(HERE / "variable_steps.npz", **variable_steps_case())
     print("wrote variable_steps")
+    np.savez_compressed(HERE / "partition.npz", **partition_case())
+    print("wrote partition")
 
 
 if __name__ == "__main__":
