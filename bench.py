@@ -17,7 +17,9 @@ Four further workloads print their own lines (``--workload bifurcation``: the ~2
 transient Y-bifurcation, mixed vs FP64 per BDF2 step; ``--workload ensemble``: 12 vessels
 solved together vs one after another; ``--workload adjoint``: the adjoint gradient of the
 ~500k-node steady Y-bifurcation, checked against central differences; ``--workload smoothers``:
-the AMG smoothers compared on the headline tube); the default is the headline above. ``--smoother chebyshev`` runs the headline with the Chebyshev smoother.
+the AMG smoothers compared on the headline tube; ``--workload partitioned``: the partitioned
+solve of 2 and 4 partitions sharing the GPU against the single-GPU solve on the headline tube);
+the default is the headline above. ``--smoother chebyshev`` runs the headline with the Chebyshev smoother.
 """
 
 from __future__ import annotations
@@ -476,6 +478,59 @@ def smoothers_workload(args):
                           "converged": rep["converged"]}), flush=True)
 
 
+def partitioned_workload(args):
+    """The partitioned solve (partitions sharing this GPU, the reference's own test setting)
+    against the single-GPU solve on the headline tube: per partition count (0 is the single-GPU
+    solver, with the partitioned solver's aggregate rebuild every 10 set-ups), the set-up time,
+    the partition report, the mean outer-iteration time and Krylov steps of iterations 4-11
+    (host clock around synchronised iterations), and the steady solve to 1e-8 from scratch with
+    its relative L2 field difference from the single-GPU solve. One JSON line per count."""
+    import torch
+
+    from zvcfd_b200.multi import B200MultiSolver
+    from zvcfd_b200.solver import B200Solver
+
+    m, fl, bcs = make_case(args.axial)
+    single = None
+    for parts in [0] + [int(p) for p in args.parts.split(",") if p]:
+        def build():
+            if parts == 0:
+                return B200Solver(m, fl, bcs, linear="b200", linear_rtol=0.1,
+                                  linear_options={"rebuild_every": 10})
+            return B200MultiSolver(m, fl, bcs, parts=parts, linear="b200", linear_rtol=0.1)
+
+        t0 = time.perf_counter()
+        s = build()
+        torch.cuda.synchronize()
+        setup = time.perf_counter() - t0
+        report = getattr(s, "report", None)
+        for _ in range(3):
+            s.iterate()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        its = [s.iterate()["linear_iterations"] for _ in range(8)]
+        torch.cuda.synchronize()
+        per = (time.perf_counter() - t) / 8
+        s.close()
+        s2 = build()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rep = s2.solve(max_iterations=150, tol=1e-8)
+        torch.cuda.synchronize()
+        to_tol = time.perf_counter() - t0
+        f = s2.fields()
+        s2.close()
+        if single is None:
+            single = f
+        err = {k: float(np.linalg.norm(f[k] - single[k]) / np.linalg.norm(single[k]))
+               for k in ("U", "P")}
+        print(json.dumps({"workload": WORKLOAD, "parts": parts, "setup_s": setup,
+                          "report": report, "ms_per_outer_iteration": per * 1e3,
+                          "krylov_steps": its, "to_1e-8_s": to_tol,
+                          "outer_iterations": rep["iterations"], "converged": rep["converged"],
+                          "field_rel_l2_vs_single": err}), flush=True)
+
+
 def adjoint_workload(args):
     """The adjoint workload: the Y-bifurcation coarsened to about 500k nodes, steady,
     Carreau-Yasuda blood, a 1 ml/s inlet and RCR outlets (Rp 1e8, C 1e-9, Rd 1e9), a fixed
@@ -805,10 +860,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stages", action="store_true")
     ap.add_argument("--workload", default="tube",
-                    choices=["tube", "bifurcation", "ensemble", "adjoint", "smoothers"],
+                    choices=["tube", "bifurcation", "ensemble", "adjoint", "smoothers",
+                             "partitioned"],
                     help="tube: the headline (default); bifurcation: the 2M-node transient; "
                          "ensemble: the 12-vessel batch; adjoint: the 500k-node steady "
-                         "gradient; smoothers: the AMG smoothers compared on the headline tube")
+                         "gradient; smoothers: the AMG smoothers compared on the headline tube; "
+                         "partitioned: partitions sharing the GPU vs the single-GPU solve")
+    ap.add_argument("--parts", default="2,4", help="partitioned workload: partition counts")
     ap.add_argument("--nodes", type=int, default=2_000_000, help="bifurcation workload size")
     ap.add_argument("--loops", type=int, default=5,
                     help="bifurcation: coefficient loops per time step at most (the reference's 5)")
@@ -847,7 +905,8 @@ def main():
         torch.cuda.set_device(local)
         if rank == 0:
             {"bifurcation": bifurcation_workload, "ensemble": ensemble_workload,
-             "adjoint": adjoint_workload, "smoothers": smoothers_workload}[args.workload](args)
+             "adjoint": adjoint_workload, "smoothers": smoothers_workload,
+             "partitioned": partitioned_workload}[args.workload](args)
         return
 
     import torch
