@@ -422,6 +422,10 @@ class B200MultiSolver:
         self.mine = [p for p in range(len(self.local)) if self.rank_of[p] == self.red.rank]
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.exchange = HaloExchange(self.plan, self.rank_of, self.red, self.device)
+        # the group's first collective involves every rank (a rank without remote halo rows
+        # takes no part in the point-to-point batches, and NCCL wants the first call to be
+        # everyone's)
+        self.red.sum(torch.zeros(1, dtype=torch.float64, device=self.device))
         self._scal = torch.ones(3, dtype=torch.float64, device=self.device)
         self.parts = {p: _Part(self, self.local[p]) for p in self.mine}
         # whole control volumes at halo nodes, from their owners
