@@ -12,6 +12,10 @@
   colours as the reference's doubling ones.
 - :func:`slots` restates the slot order ``argsort(colour * E + e)`` and the
   per-colour offsets (``fast.py:199-203``).
+
+Pinned: ``tests/test_colour.py`` holds :func:`colour` to the colours of the reference's own
+``gpu_colour``, run on the CPU with its kernel source compiled by g++
+(``tests/golden/make_golden.py colour``).
 """
 
 from __future__ import annotations

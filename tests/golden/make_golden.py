@@ -19,7 +19,8 @@ the manufactured Carreau-Yasuda outlet (``gn_outlet``); developed inlet
 profiles and a pipe with the default flow-rate inlet (``profiles``); uneven BDF2 steps of
 an oscillating pipe (``variable_steps``); a mid-size curved Carreau-Yasuda tube
 (``curved_mid``, about 6k nodes, the bench tube's cross-section coarsened); Morton owners,
-local meshes and halo plans of the reference's partitioner (``partition``). A single file is
+local meshes and halo plans of the reference's partitioner (``partition``); element colours of
+the reference's device colouring ``gpu_colour`` run on the CPU (``colour``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -571,7 +572,144 @@ def partition_case() -> dict:
     return out
 
 
+# ---------------------------------------------------------------- the reference's colouring
+
+_SHIM = r"""
+// CUDA's built-ins for running a kernel's threads one after another on the CPU
+#include <stdint.h>
+struct zv_dim { long long x; };
+static zv_dim blockIdx, threadIdx, blockDim;
+#define __global__
+static inline unsigned long long atomicMin(unsigned long long *a, unsigned long long v) {
+    unsigned long long o = *a; if (v < o) *a = v; return o; }
+static inline unsigned long long atomicAdd(unsigned long long *a, unsigned long long v) {
+    unsigned long long o = *a; *a = o + v; return o; }
+static inline int __ffsll(long long v) { return __builtin_ffsll(v); }
+"""
+
+_LAUNCH = r"""
+#define ZV_GRID(call) blockDim.x = block; \
+    for (long long b = 0; b < grid; ++b) for (long long t = 0; t < block; ++t) { \
+        blockIdx.x = b; threadIdx.x = t; call; }
+extern "C" void launch_colour_claim(long long grid, long long block, const int *conn, int n,
+        long long E, const unsigned long long *key, const int *colour, unsigned long long *best) {
+    ZV_GRID(colour_claim(conn, n, E, key, colour, best)) }
+extern "C" void launch_colour_pick(long long grid, long long block, const int *conn, int n,
+        long long E, const unsigned long long *key, int *colour, const unsigned long long *best,
+        unsigned long long *used, int W, unsigned long long *ctr) {
+    ZV_GRID(colour_pick(conn, n, E, key, colour, best, used, W, ctr)) }
+"""
+
+
+def _cpu_cupy():
+    """A stand-in for the ``cupy`` module, enough for the reference's ``gpu_colour`` and
+    ``_keys`` (``zvcfd/fv/fast.py:35-130``): arrays are numpy arrays with CuPy's ``get``, and
+    ``RawKernel`` compiles the kernel source the reference hands it with g++ for the CPU
+    (``oracle/_ref/``, not committed): CUDA's built-ins become a sequential loop over the
+    grid and plain read-modify-writes. The colouring's results do not depend on the order of
+    its threads (a claim round is an ``atomicMin`` per node; a round's winners share no node),
+    so this is the colouring the reference computes on a GPU."""
+    import ctypes
+    import hashlib
+    import subprocess
+    import types
+
+    class Arr(np.ndarray):
+        def get(self):
+            return np.asarray(self)
+
+    def wrap(fn):
+        return lambda *a, **k: np.asarray(fn(*a, **k)).view(Arr)
+
+    out_dir = HERE.parents[1] / "oracle" / "_ref"
+    out_dir.mkdir(parents=True, exist_ok=True)
+
+    class RawKernel:
+        libs = {}
+
+        def __init__(self, src, name, options=()):
+            tag = hashlib.sha1(src.encode()).hexdigest()[:12]
+            if tag not in RawKernel.libs:
+                cpp, so = out_dir / f"colour_{tag}.cpp", out_dir / f"colour_{tag}.so"
+                cpp.write_text(_SHIM + src + _LAUNCH)
+                subprocess.run(["g++", "-O2", "-shared", "-fPIC", "-o", str(so), str(cpp)],
+                               check=True)
+                RawKernel.libs[tag] = ctypes.CDLL(str(so))
+            self.fn = getattr(RawKernel.libs[tag], f"launch_{name}")
+
+        def __call__(self, grid, block, args):
+            conv = []
+            for a in args:
+                if isinstance(a, np.ndarray):
+                    conv.append(ctypes.c_void_p(a.ctypes.data))
+                elif isinstance(a, np.int32):
+                    conv.append(ctypes.c_int(int(a)))
+                else:
+                    conv.append(ctypes.c_longlong(int(a)))
+            self.fn(ctypes.c_longlong(grid[0]), ctypes.c_longlong(block[0]), *conv)
+
+    cp = types.ModuleType("cupy")
+    cp.uint64, cp.int32, cp.int64 = np.uint64, np.int32, np.int64
+    for name in ("arange", "ascontiguousarray", "empty", "zeros", "full"):
+        setattr(cp, name, wrap(getattr(np, name)))
+    cp.cuda = types.SimpleNamespace(Device=lambda *a: types.SimpleNamespace(id=0))
+    cp.RawKernel = RawKernel
+    return cp
+
+
+def box_tets(n):
+    """Five tetrahedra per cube of an n^3 grid of cubes (the reference's
+    ``tests/test_fv_fast.py:59-69`` mesh)."""
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+
+    def v(a, b, c):
+        return ((i + a) * (n + 1) + (j + b)) * (n + 1) + (k + c)
+
+    c = [v(0, 0, 0), v(1, 0, 0), v(1, 1, 0), v(0, 1, 0), v(0, 0, 1), v(1, 0, 1), v(1, 1, 1),
+         v(0, 1, 1)]
+    tets = [(0, 1, 3, 4), (1, 2, 3, 6), (1, 4, 5, 6), (3, 4, 6, 7), (1, 3, 4, 6)]
+    return np.stack([np.stack([c[t].ravel() for t in tet], 1) for tet in tets], 0) \
+        .reshape(-1, 4).astype(np.int32), (n + 1) ** 3
+
+
+def colour_case() -> dict:
+    """The reference's ``gpu_colour`` (run on the CPU, :func:`_cpu_cupy`) on the meshes the
+    device colouring is tested on: a jittered tetrahedral pipe, the hexahedra and wedges of a
+    curved tube, a box of 40,960 tetrahedra, the six kernel meshes, and a fan of 200 tetrahedra
+    on one node coloured with one 64-bit mask word (the masks widen twice)."""
+    sys.modules["cupy"] = _cpu_cupy()
+    from zvcfd.fv.fast import gpu_colour
+
+    out = {}
+    cases = {}
+    pm = zmesh.pipe(1.0, 3.0, n_core=4, n_ring=3, n_axial=10, kind="tet", jitter_amount=0.1,
+                    seed=3)
+    cm = zmesh.curved_tube(1.0, 5.0, n_core=4, n_ring=4, n_axial=12, layers=2)
+    for tag, m in (("pipe", pm), ("curved", cm)):
+        for k, e in m.elements.items():
+            cases[f"{tag}_{k}"] = (e, m.n_nodes, 4)
+    for name, make in MESHES.items():
+        m = make()
+        for k, e in m.elements.items():
+            cases[f"kernel_{name}_{k}"] = (e, m.n_nodes, 4)
+    cases["box16"] = box_tets(16) + (4,)
+    fan = np.column_stack([np.zeros(200, np.int64), 3 * np.arange(200) + 1,
+                           3 * np.arange(200) + 2, 3 * np.arange(200) + 3])
+    cases["fan"] = (fan, 601, 1)
+    for tag, (e, n, words) in cases.items():
+        col = np.asarray(gpu_colour(np.asarray(e), n, words=words))
+        out[f"{tag}_conn"] = np.asarray(e, np.int32) if tag != "box16" else np.zeros(0)
+        out[f"{tag}_meta"] = np.array([n, words])
+        out[f"{tag}_colour"] = col.astype(np.int32)
+    out["cases"] = np.array(sorted(cases))
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["colour"]:
+        np.savez_compressed(HERE / "colour.npz", **colour_case())
+        print("wrote colour")
+        return
     if sys.argv[1:] == ["partition"]:
         np.savez_compressed(HERE / "partition.npz", **partition_case())
         print("wrote partition")
@@ -657,6 +795,8 @@ def main():
     print("wrote variable_steps")
     np.savez_compressed(HERE / "partition.npz", **partition_case())
     print("wrote partition")
+    np.savez_compressed(HERE / "colour.npz", **colour_case())
+    print("wrote colour")
 
 
 if __name__ == "__main__":
