@@ -2,6 +2,11 @@
 
 - :func:`bsr_matvec` restates ``bsr_mv`` + ``BlockMatrix.matvec`` (``zvcfd/fv/linear.py:47-61``,
   ``:93-103``): ``y = A x + sum u (w . x)`` with SciPy's block-CSR product.
+
+Pinned: ``tests/test_acm_reference.py`` holds :class:`ACM` (at the reference's parameters) and
+:func:`fgmres` to the reference's own ACM and device FGMRES, run on the CPU
+(``tests/golden/make_golden.py acm``): the same aggregates bit for bit, the same Krylov
+iteration counts, V-cycles and solutions to 1e-14 and 1e-13.
 """
 
 from __future__ import annotations

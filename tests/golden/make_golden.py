@@ -20,7 +20,9 @@ profiles and a pipe with the default flow-rate inlet (``profiles``); uneven BDF2
 an oscillating pipe (``variable_steps``); a mid-size curved Carreau-Yasuda tube
 (``curved_mid``, about 6k nodes, the bench tube's cross-section coarsened); Morton owners,
 local meshes and halo plans of the reference's partitioner (``partition``); element colours of
-the reference's device colouring ``gpu_colour`` run on the CPU (``colour``). A single file is
+the reference's device colouring ``gpu_colour`` run on the CPU (``colour``); the reference's ACM
+levels, V-cycle and ACM-FGMRES solve on a system its CPU solver assembled (``acm``). A single
+file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -587,28 +589,48 @@ static inline unsigned long long atomicAdd(unsigned long long *a, unsigned long 
 static inline int __ffsll(long long v) { return __builtin_ffsll(v); }
 """
 
-_LAUNCH = r"""
-#define ZV_GRID(call) blockDim.x = block; \
-    for (long long b = 0; b < grid; ++b) for (long long t = 0; t < block; ++t) { \
-        blockIdx.x = b; threadIdx.x = t; call; }
-extern "C" void launch_colour_claim(long long grid, long long block, const int *conn, int n,
-        long long E, const unsigned long long *key, const int *colour, unsigned long long *best) {
-    ZV_GRID(colour_claim(conn, n, E, key, colour, best)) }
-extern "C" void launch_colour_pick(long long grid, long long block, const int *conn, int n,
-        long long E, const unsigned long long *key, int *colour, const unsigned long long *best,
-        unsigned long long *used, int W, unsigned long long *ctr) {
-    ZV_GRID(colour_pick(conn, n, E, key, colour, best, used, W, ctr)) }
-"""
+def _launcher(src: str, name: str) -> str:
+    """A C function ``launch_<name>(grid, block, <the kernel's parameters>)`` running the
+    kernel's threads one after another over the grid."""
+    import re
+
+    m = re.search(r"__global__\s+void\s+" + name + r"\s*\(([^)]*)\)", src)
+    params = [p.strip() for p in m.group(1).split(",")]
+    names = [re.findall(r"[A-Za-z_]\w*", p)[-1] for p in params]
+    return (f'extern "C" void launch_{name}(long long grid, long long block, '
+            f'{", ".join(params)}) {{\n    blockDim.x = block;\n'
+            f"    for (long long b = 0; b < grid; ++b) for (long long t = 0; t < block; ++t) "
+            f"{{ blockIdx.x = b; threadIdx.x = t; {name}({', '.join(names)}); }}\n}}\n")
+
+
+def _ctypes_of(src: str, name: str) -> list:
+    import ctypes
+    import re
+
+    m = re.search(r"__global__\s+void\s+" + name + r"\s*\(([^)]*)\)", src)
+    out = []
+    for p in (q.strip() for q in m.group(1).split(",")):
+        if "*" in p:
+            out.append(ctypes.c_void_p)
+        elif "long long" in p:
+            out.append(ctypes.c_longlong)
+        elif "double" in p:
+            out.append(ctypes.c_double)
+        else:
+            out.append(ctypes.c_int)
+    return out
 
 
 def _cpu_cupy():
-    """A stand-in for the ``cupy`` module, enough for the reference's ``gpu_colour`` and
-    ``_keys`` (``zvcfd/fv/fast.py:35-130``): arrays are numpy arrays with CuPy's ``get``, and
-    ``RawKernel`` compiles the kernel source the reference hands it with g++ for the CPU
-    (``oracle/_ref/``, not committed): CUDA's built-ins become a sequential loop over the
-    grid and plain read-modify-writes. The colouring's results do not depend on the order of
-    its threads (a claim round is an ``atomicMin`` per node; a round's winners share no node),
-    so this is the colouring the reference computes on a GPU."""
+    """A stand-in for the ``cupy`` module on the CPU, enough for the reference's device
+    colouring (``zvcfd/fv/fast.py:35-130``), its ``BlockMatrix`` product and its ACM and
+    FGMRES (``zvcfd/fv/linear.py:47-135``, ``:238-518``): arrays are numpy arrays with CuPy's
+    ``get``; array functions are numpy's; ``RawKernel`` compiles the kernel source the
+    reference hands it with g++ for the CPU (``oracle/_ref/``, not committed), CUDA's built-ins
+    made a sequential loop over the grid and plain read-modify-writes. These kernels' results
+    do not depend on the order of their threads (one thread per block row for the product; for
+    the colouring an ``atomicMin`` claim per node and winners that share no node), so they are
+    what the reference computes on a GPU."""
     import ctypes
     import hashlib
     import subprocess
@@ -628,30 +650,36 @@ def _cpu_cupy():
         libs = {}
 
         def __init__(self, src, name, options=()):
-            tag = hashlib.sha1(src.encode()).hexdigest()[:12]
+            tag = hashlib.sha1((src + name).encode()).hexdigest()[:12]
             if tag not in RawKernel.libs:
-                cpp, so = out_dir / f"colour_{tag}.cpp", out_dir / f"colour_{tag}.so"
-                cpp.write_text(_SHIM + src + _LAUNCH)
+                cpp, so = out_dir / f"kernel_{tag}.cpp", out_dir / f"kernel_{tag}.so"
+                cpp.write_text(_SHIM + src + _launcher(src, name))
                 subprocess.run(["g++", "-O2", "-shared", "-fPIC", "-o", str(so), str(cpp)],
                                check=True)
                 RawKernel.libs[tag] = ctypes.CDLL(str(so))
             self.fn = getattr(RawKernel.libs[tag], f"launch_{name}")
+            self.types = _ctypes_of(src, name)
 
         def __call__(self, grid, block, args):
-            conv = []
-            for a in args:
-                if isinstance(a, np.ndarray):
-                    conv.append(ctypes.c_void_p(a.ctypes.data))
-                elif isinstance(a, np.int32):
-                    conv.append(ctypes.c_int(int(a)))
-                else:
-                    conv.append(ctypes.c_longlong(int(a)))
+            conv = [ctypes.c_void_p(np.ascontiguousarray(a).ctypes.data) if t is ctypes.c_void_p
+                    else t(a) for a, t in zip(args, self.types)]
+            for a, t in zip(args, self.types):
+                if t is ctypes.c_void_p and not a.flags.c_contiguous:
+                    raise ValueError("a kernel argument must be contiguous")
             self.fn(ctypes.c_longlong(grid[0]), ctypes.c_longlong(block[0]), *conv)
 
-    cp = types.ModuleType("cupy")
-    cp.uint64, cp.int32, cp.int64 = np.uint64, np.int32, np.int64
-    for name in ("arange", "ascontiguousarray", "empty", "zeros", "full"):
+    class CuPy(types.ModuleType):
+        def __getattr__(self, name):
+            return getattr(np, name)
+
+    cp = CuPy("cupy")
+    for name in ("arange", "ascontiguousarray", "asarray", "empty", "zeros", "ones", "full",
+                 "zeros_like", "empty_like", "concatenate", "stack", "searchsorted",
+                 "flatnonzero", "cumsum", "bincount", "argsort", "sqrt", "dot", "einsum"):
         setattr(cp, name, wrap(getattr(np, name)))
+    cp.asnumpy = np.asarray
+    cp.ndarray = np.ndarray
+    cp.linalg = types.SimpleNamespace(inv=wrap(np.linalg.inv), norm=np.linalg.norm)
     cp.cuda = types.SimpleNamespace(Device=lambda *a: types.SimpleNamespace(id=0))
     cp.RawKernel = RawKernel
     return cp
@@ -705,7 +733,70 @@ def colour_case() -> dict:
     return out
 
 
+def acm_case() -> dict:
+    """The reference's own ACM (``zvcfd/fv/linear.py:328-518``) and device FGMRES
+    (``:238-320``), run on the CPU through :func:`_cpu_cupy`, on a system the reference's CPU
+    solver assembled: the golden tetrahedral pipe after three Picard iterations (Dirichlet rows
+    in place), with ``coarse=40`` (one coarse level) and ``coarse=8`` (deeper). Recorded: the
+    system, and per setting each
+    level's aggregates and Galerkin operator, one V-cycle of the right-hand side, and the
+    ACM-FGMRES solve to 1e-10 (solution, iterations, residual)."""
+    sys.modules["cupy"] = _cpu_cupy()
+    import scipy.sparse as sp  # noqa: F401
+
+    from zvcfd.fv.linear import ACM, BlockMatrix
+
+    g = np.load(HERE / "pipe_tet_si.npz")
+    nodes = g["nodes"]
+    elements = {k: g[f"elem_{k}"] for k in ("tet", "pyramid", "wedge", "hex") if f"elem_{k}" in g}
+    pm = zmesh.Mesh(nodes, elements)
+    for zid, name in zip(g["zone_ids"], g["zone_names"]):
+        pm.zones[int(zid)] = zmesh.Zone(int(zid), "", str(name), g[f"zone_{int(zid)}"])
+    um = to_reference(pm)
+    z = {zz.name: k for k, zz in pm.zones.items()}
+    R2 = float(g["radius"])
+
+    def prof(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R2 ** 2
+        return np.stack([0 * r2, 0 * r2, 0.2 * np.clip(1 - r2, 0, None)], 1)
+
+    bcs = {z["inlet"]: {"kind": "velocity", "value": prof},
+           z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}}
+    s = ReferenceSolver(um, Fluid(1060.0, 3.5e-3), bcs, advection=1.0, lag_rhie_chow=True)
+    s.solve(max_iterations=3, tol=0.0)
+    M, b = s.assemble()
+    indptr, indices = node_graph(um)
+    data = blocks_on_pattern(M, indptr, indices)
+    A = BlockMatrix(np.asarray(indptr, np.int64), np.asarray(indices, np.int32), data)
+    out = {"indptr": A.indptr, "indices": A.indices, "data": data, "b": b,
+           "coarse": np.array([40, 8])}
+    for coarse in (40, 8):
+        acm = ACM(coarse=coarse)
+        acm.setup(A)
+        pre = f"c{coarse}_"
+        out[pre + "levels"] = np.array(len(acm.levels))
+        for i, L in enumerate(acm.levels):
+            out[f"{pre}level{i}_n"] = np.array(L["A"].n)
+            out[f"{pre}level{i}_dense"] = np.array("dense_inv" in L)
+            if "agg" in L:
+                out[f"{pre}level{i}_agg"] = np.asarray(L["agg"])
+            if i:
+                out[f"{pre}level{i}_indptr"] = np.asarray(L["A"].indptr)
+                out[f"{pre}level{i}_indices"] = np.asarray(L["A"].indices)
+                out[f"{pre}level{i}_data"] = np.asarray(L["A"].data)
+        out[pre + "vcycle"] = np.asarray(acm.vcycle(np.asarray(b).copy()))
+        x, info = acm.solve(A, np.asarray(b).copy(), rtol=1e-10)
+        out.update({pre + "x": np.asarray(x), pre + "iterations": np.array(info.iterations),
+                    pre + "residual": np.array(info.residual),
+                    pre + "converged": np.array(info.converged)})
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["acm"]:
+        np.savez_compressed(HERE / "acm.npz", **acm_case())
+        print("wrote acm")
+        return
     if sys.argv[1:] == ["colour"]:
         np.savez_compressed(HERE / "colour.npz", **colour_case())
         print("wrote colour")
@@ -797,6 +888,8 @@ def main():
     print("wrote partition")
     np.savez_compressed(HERE / "colour.npz", **colour_case())
     print("wrote colour")
+    np.savez_compressed(HERE / "acm.npz", **acm_case())
+    print("wrote acm")
 
 
 if __name__ == "__main__":
