@@ -21,8 +21,8 @@ an oscillating pipe (``variable_steps``); a mid-size curved Carreau-Yasuda tube
 (``curved_mid``, about 6k nodes, the bench tube's cross-section coarsened); Morton owners,
 local meshes and halo plans of the reference's partitioner (``partition``); element colours of
 the reference's device colouring ``gpu_colour`` run on the CPU (``colour``); the reference's ACM
-levels, V-cycle and ACM-FGMRES solve on a system its CPU solver assembled (``acm``). A single
-file is
+levels, V-cycle and ACM-FGMRES solve on a system its CPU solver assembled (``acm``); its
+device boundary pass run on the CPU (``boundary``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -577,11 +577,20 @@ def partition_case() -> dict:
 # ---------------------------------------------------------------- the reference's colouring
 
 _SHIM = r"""
-// CUDA's built-ins for running a kernel's threads one after another on the CPU
+// CUDA's built-ins for running a kernel's threads on the CPU: one after another, or, for a
+// kernel with block barriers, each block's threads as OpenMP threads (__syncthreads an
+// OpenMP barrier, __shared__ storage static: blocks run one at a time)
 #include <stdint.h>
+#include <math.h>
+#include <omp.h>
 struct zv_dim { long long x; };
-static zv_dim blockIdx, threadIdx, blockDim;
+static zv_dim blockIdx, blockDim;
+static thread_local zv_dim threadIdx;
 #define __global__
+#define __shared__ static
+static inline void __syncthreads() {
+    _Pragma("omp barrier")
+}
 static inline unsigned long long atomicMin(unsigned long long *a, unsigned long long v) {
     unsigned long long o = *a; if (v < o) *a = v; return o; }
 static inline unsigned long long atomicAdd(unsigned long long *a, unsigned long long v) {
@@ -597,10 +606,17 @@ def _launcher(src: str, name: str) -> str:
     m = re.search(r"__global__\s+void\s+" + name + r"\s*\(([^)]*)\)", src)
     params = [p.strip() for p in m.group(1).split(",")]
     names = [re.findall(r"[A-Za-z_]\w*", p)[-1] for p in params]
-    return (f'extern "C" void launch_{name}(long long grid, long long block, '
-            f'{", ".join(params)}) {{\n    blockDim.x = block;\n'
-            f"    for (long long b = 0; b < grid; ++b) for (long long t = 0; t < block; ++t) "
-            f"{{ blockIdx.x = b; threadIdx.x = t; {name}({', '.join(names)}); }}\n}}\n")
+    head = (f'extern "C" void launch_{name}(long long grid, long long block, '
+            f'{", ".join(params)}) {{\n    blockDim.x = block;\n')
+    call = f"{name}({', '.join(names)});"
+    if "__syncthreads" in src:
+        return (head + "    omp_set_dynamic(0);\n"
+                "    for (long long zv_b = 0; zv_b < grid; ++zv_b) {\n"
+                "        blockIdx.x = zv_b;\n#pragma omp parallel num_threads((int)block)\n"
+                f"        {{ threadIdx.x = omp_get_thread_num(); {call} }}\n    }}\n}}\n")
+    return (head + "    for (long long zv_b = 0; zv_b < grid; ++zv_b) "
+            "for (long long zv_t = 0; zv_t < block; ++zv_t) "
+            f"{{ blockIdx.x = zv_b; threadIdx.x = zv_t; {call} }}\n}}\n")
 
 
 def _ctypes_of(src: str, name: str) -> list:
@@ -654,8 +670,8 @@ def _cpu_cupy():
             if tag not in RawKernel.libs:
                 cpp, so = out_dir / f"kernel_{tag}.cpp", out_dir / f"kernel_{tag}.so"
                 cpp.write_text(_SHIM + src + _launcher(src, name))
-                subprocess.run(["g++", "-O2", "-shared", "-fPIC", "-o", str(so), str(cpp)],
-                               check=True)
+                subprocess.run(["g++", "-O2", "-fopenmp", "-shared", "-fPIC", "-o", str(so),
+                                str(cpp)], check=True)
                 RawKernel.libs[tag] = ctypes.CDLL(str(so))
             self.fn = getattr(RawKernel.libs[tag], f"launch_{name}")
             self.types = _ctypes_of(src, name)
@@ -792,7 +808,78 @@ def acm_case() -> dict:
     return out
 
 
+def boundary_case() -> dict:
+    """The reference's boundary pass (its ``finalise`` kernel, ``zvcfd/fv/_cuda_bc.py:32-138``)
+    run on the CPU (:func:`_cpu_cupy`) on the raw system the oracle assembles for the golden
+    tetrahedral pipe after three outer iterations with a false time step, with and without
+    elimination. The pass's own known terms (time, body force, outlet force, inflow, outflow
+    momentum, lumped rows) are given as zeros, since the raw system holds them: so this is the
+    part the oracle's ``boundary_pass`` restates (Dirichlet rows, elimination, residual
+    statistics, row scaling). Recorded: the inputs, and per case the scaled blocks, right-hand
+    side, row scales and the residual maxima per equation. Not the sums of squares: the
+    kernel's partial-sum tree has the four threads of a row add the same pair, which a GPU
+    warp, in lockstep, performs once and concurrent CPU threads do not."""
+    import ctypes  # noqa: F401
+
+    cp = _cpu_cupy()
+    from zvcfd.fv._cuda_bc import FINALISE
+
+    from oracle.fv import OracleSolver
+    sys.path.insert(0, str(HERE.parent))
+    from fixtures import fluid_of, load, mesh_of, pipe_bcs
+
+    out = {}
+    name = "pipe_tet_si"
+    g = load(name)
+    m = mesh_of(g)
+    fl = fluid_of(g)
+    kernel = cp.RawKernel(FINALISE, "finalise")
+    for dt in (0.02,):
+        o = OracleSolver(m, fl, pipe_bcs(name, g, m), advection=1.0, dt=dt)
+        o.solve(max_iterations=3, tol=0.0)
+        o.momentum_diagonal()
+        o.assemble()
+        raw, braw = o.raw
+        N = o.N
+        X = np.concatenate([o.U, o.P[:, None]], 1)
+        tag = "dt" if dt else "steady"
+        fixed = np.concatenate([o.vel_fixed_comp, o.p_fixed[:, None]], 1)
+        uref = max(np.abs(o.U).max(), np.abs(o.vel_value).max(), 1e-30)
+        pref = max(np.ptp(o.P), fl.rho * uref * uref, 1e-30)
+        out.update({f"{tag}_indptr": o.indptr, f"{tag}_indices": o.indices,
+                    f"{tag}_raw": raw, f"{tag}_braw": braw.reshape(N, 4), f"{tag}_x": X,
+                    f"{tag}_fixed": fixed, f"{tag}_vel": o.vel_value, f"{tag}_pval": o.p_value,
+                    f"{tag}_aP": o.aP, f"{tag}_V": o.V, f"{tag}_U": o.U, f"{tag}_P": o.P,
+                    f"{tag}_rho": np.array(fl.rho)})
+        rows = np.repeat(np.arange(N), np.diff(o.indptr))
+        dpos = np.flatnonzero(rows == o.indices).astype(np.int64)
+        zN, zN3 = np.zeros(N), np.zeros((N, 3))
+        for elim in (1, 0):
+            data = np.ascontiguousarray(raw, np.float64).copy()
+            b = np.ascontiguousarray(braw.reshape(-1), np.float64).copy()
+            nb = (4 * N + 255) // 256
+            rs = np.zeros(4 * N)
+            partial = np.zeros(nb * 8)
+            kernel((nb,), (256,), (
+                np.int64(N), np.asarray(o.indptr, np.int64), np.asarray(o.indices, np.int32),
+                dpos, data, b, np.int32(0), zN, zN3, zN3, zN3, zN, zN, zN, zN, zN, np.int32(1),
+                zN3, fixed.astype(np.uint8), fixed.astype(np.uint8), o.vel_value.copy(),
+                o.p_value.copy(), np.int32(elim), np.full(N, -1, np.int64), np.zeros(16),
+                np.zeros(4 * N), X.reshape(-1).copy(), o.aP.copy(), o.V.copy(),
+                np.float64(fl.rho), np.array([uref, pref, np.abs(o.U).max()]), zN, rs,
+                partial))
+            part = partial.reshape(nb, 8)
+            key = f"{tag}_e{elim}"
+            out.update({f"{key}_data": data, f"{key}_b": b.reshape(N, 4),
+                        f"{key}_scale": rs.reshape(N, 4), f"{key}_max": part[:, 4:].max(0)})
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["boundary"]:
+        np.savez_compressed(HERE / "boundary_pass.npz", **boundary_case())
+        print("wrote boundary_pass")
+        return
     if sys.argv[1:] == ["acm"]:
         np.savez_compressed(HERE / "acm.npz", **acm_case())
         print("wrote acm")
@@ -890,6 +977,8 @@ def main():
     print("wrote colour")
     np.savez_compressed(HERE / "acm.npz", **acm_case())
     print("wrote acm")
+    np.savez_compressed(HERE / "boundary_pass.npz", **boundary_case())
+    print("wrote boundary_pass")
 
 
 if __name__ == "__main__":
