@@ -225,6 +225,18 @@ def fgmres(matvec, precond, b, x0, *, rtol: float, restart: int = 30, maxiter: i
 
 # ---------------------------------------------------------------- one partition
 
+def _node_view(name):
+    """A property: the global boundary's node array ``name`` at a partition's local nodes."""
+    return property(lambda self: getattr(self.g, name)[self.idx])
+
+
+def _face_view(name):
+    """A property: the global boundary's per-face dict ``name`` at the faces a partition
+    holds."""
+    return property(lambda self: {z: None if v is None else v[self.lm.faces[z]]
+                                  for z, v in getattr(self.g, name).items()})
+
+
 class PartBoundary:
     """The global :class:`~zvcfd_b200.boundary.Boundary` seen from one partition.
 
@@ -246,20 +258,13 @@ class PartBoundary:
         self.zone_nodes = {zid: np.unique(f[f >= 0]) for zid, (f, _) in self.sub.items()}
         self.pin = None
 
-    def _node(name):                                           # noqa: N805
-        return property(lambda self: getattr(self.g, name)[self.idx])
-
-    wall, inlet, outlet, sym = _node("wall"), _node("inlet"), _node("outlet"), _node("sym")
-    vel_fixed, vel_fixed_comp = _node("vel_fixed"), _node("vel_fixed_comp")
-    p_fixed, vel_value, p_value, inflow = (_node("p_fixed"), _node("vel_value"),
-                                           _node("p_value"), _node("inflow"))
-
-    def _faces(name):                                          # noqa: N805
-        return property(lambda self: {z: None if v is None else v[self.lm.faces[z]]
-                                      for z, v in getattr(self.g, name).items()})
-
-    sub_flow, sub_vel, p_sub, p_grad = (_faces("sub_flow"), _faces("sub_vel"),
-                                        _faces("p_sub"), _faces("p_grad"))
+    wall, inlet = _node_view("wall"), _node_view("inlet")
+    outlet, sym = _node_view("outlet"), _node_view("sym")
+    vel_fixed, vel_fixed_comp = _node_view("vel_fixed"), _node_view("vel_fixed_comp")
+    p_fixed, vel_value = _node_view("p_fixed"), _node_view("vel_value")
+    p_value, inflow = _node_view("p_value"), _node_view("inflow")
+    sub_flow, sub_vel = _face_view("sub_flow"), _face_view("sub_vel")
+    p_sub, p_grad = _face_view("p_sub"), _face_view("p_grad")
 
     def _global(self, key, fn):
         if key not in self.cache:
