@@ -702,7 +702,6 @@ class B200MultiSolver:
                     "linear_setup_s": info.setup_seconds, "linear_solve_s": info.seconds,
                     "seconds": time.time() - t0, "imbalance": sum(q.values()) / gross,
                     "flows": q})
-        self._flows = q
         self.iteration += 1
         return rec
 
