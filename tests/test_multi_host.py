@@ -207,3 +207,27 @@ def test_partition_boundary_sums_to_the_global_boundary():
                                                    -1), gf)
     np.testing.assert_allclose(W_sum, W, atol=1e-15)
     np.testing.assert_allclose(c_sum, c, rtol=1e-12, atol=1e-15 * np.abs(c).max())
+
+
+def test_fgmres_edge_cases():
+    """The stopping rules shared with the device FGMRES: nothing to do, a lucky breakdown,
+    the step budget, restarts."""
+    rng = np.random.default_rng(4)
+    ident = lambda v: v.clone()                                    # noqa: E731
+    z = torch.zeros(12, dtype=torch.float64)
+    x, it, res, ok = fgmres(ident, ident, z, z, rtol=1e-8)
+    assert it == 0 and ok and res == 0.0 and not x.any()           # b = 0, x0 = 0
+    b = torch.as_tensor(rng.normal(size=12))
+    x, it, res, ok = fgmres(ident, ident, b, z, rtol=1e-12)
+    assert it == 1 and ok                                          # exact after one step
+    np.testing.assert_allclose(x.numpy(), b.numpy(), rtol=0, atol=1e-15 * b.abs().max().item())
+    M = torch.as_tensor(np.diag(np.linspace(1.0, 100.0, 40)) + 0.3 * np.eye(40, k=1))
+    b = torch.as_tensor(rng.normal(size=40))
+    x, it, res, ok = fgmres(lambda v: M @ v, ident, b, torch.zeros(40, dtype=torch.float64),
+                            rtol=1e-10, maxiter=3)
+    assert it == 3 and not ok and res > 1e-10
+    x, it, res, ok = fgmres(lambda v: M @ v, ident, b, torch.zeros(40, dtype=torch.float64),
+                            rtol=1e-10, restart=5, maxiter=400)
+    assert ok and it > 5 and res <= 1.01e-10
+    want = np.linalg.solve(M.numpy(), b.numpy())
+    assert np.abs(x.numpy() - want).max() <= 1e-8 * np.abs(want).max()
