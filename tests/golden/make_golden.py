@@ -22,7 +22,8 @@ an oscillating pipe (``variable_steps``); a mid-size curved Carreau-Yasuda tube
 local meshes and halo plans of the reference's partitioner (``partition``); element colours of
 the reference's device colouring ``gpu_colour`` run on the CPU (``colour``); the reference's ACM
 levels, V-cycle and ACM-FGMRES solve on a system its CPU solver assembled (``acm``); its
-device boundary pass run on the CPU (``boundary``). A single file is
+device boundary pass run on the CPU (``boundary``); its whole device solver run on the CPU for
+the RCR outlet, the average-pressure outlet and the opening (``gpu_path``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -588,8 +589,23 @@ static zv_dim blockIdx, blockDim;
 static thread_local zv_dim threadIdx;
 #define __global__
 #define __shared__ static
+#define __constant__ static const
+#define __device__
 static inline void __syncthreads() {
     _Pragma("omp barrier")
+}
+struct double2 { double x, y; };
+static inline double2 make_double2(double a, double b) { double2 r; r.x = a; r.y = b; return r; }
+// a warp shuffle over the block's threads (all of them call it, as the kernels do): values
+// exchanged through a block-wide buffer between two barriers
+static double zv_shfl[1024];
+static inline double __shfl_down_sync(unsigned mask, double v, int delta, int width) {
+    int t = (int)threadIdx.x;
+    zv_shfl[t] = v;
+    _Pragma("omp barrier")
+    double r = (t % width + delta < width) ? zv_shfl[t + delta] : v;
+    _Pragma("omp barrier")
+    return r;
 }
 static inline unsigned long long atomicMin(unsigned long long *a, unsigned long long v) {
     unsigned long long o = *a; if (v < o) *a = v; return o; }
@@ -609,7 +625,7 @@ def _launcher(src: str, name: str) -> str:
     head = (f'extern "C" void launch_{name}(long long grid, long long block, '
             f'{", ".join(params)}) {{\n    blockDim.x = block;\n')
     call = f"{name}({', '.join(names)});"
-    if "__syncthreads" in src:
+    if "__syncthreads" in src or "__shfl" in src:
         return (head + "    omp_set_dynamic(0);\n"
                 "    for (long long zv_b = 0; zv_b < grid; ++zv_b) {\n"
                 "        blockIdx.x = zv_b;\n#pragma omp parallel num_threads((int)block)\n"
@@ -638,15 +654,18 @@ def _ctypes_of(src: str, name: str) -> list:
 
 
 def _cpu_cupy():
-    """A stand-in for the ``cupy`` module on the CPU, enough for the reference's device
-    colouring (``zvcfd/fv/fast.py:35-130``), its ``BlockMatrix`` product and its ACM and
-    FGMRES (``zvcfd/fv/linear.py:47-135``, ``:238-518``): arrays are numpy arrays with CuPy's
-    ``get``; array functions are numpy's; ``RawKernel`` compiles the kernel source the
-    reference hands it with g++ for the CPU (``oracle/_ref/``, not committed), CUDA's built-ins
-    made a sequential loop over the grid and plain read-modify-writes. These kernels' results
-    do not depend on the order of their threads (one thread per block row for the product; for
-    the colouring an ``atomicMin`` claim per node and winners that share no node), so they are
-    what the reference computes on a GPU."""
+    """A stand-in for the ``cupy`` module on the CPU, enough for the reference's device path:
+    its colouring (``zvcfd/fv/fast.py:35-130``), ``BlockMatrix`` product, ACM and FGMRES
+    (``zvcfd/fv/linear.py:47-135``, ``:238-518``), fast element kernels
+    (``zvcfd/fv/_cuda_fast.py``), boundary pass (``zvcfd/fv/_cuda_bc.py``) and so its whole
+    ``GPUSolver``. Arrays are numpy arrays with CuPy's ``get``; array functions are numpy's;
+    ``RawKernel``/``RawModule`` compile the kernel source the reference hands them with g++ for
+    the CPU (``oracle/_ref/``, not committed): a kernel without block barriers or shuffles runs
+    its threads one after another, one with them runs each block's threads as OpenMP threads
+    (``_SHIM``). The kernels' results do not depend on the order of their threads (one writer
+    per address: a thread per block row, colour-ordered element scatters, an ``atomicMin`` claim
+    per node), so they are what the reference computes on a GPU, with one exception: the
+    residual sums of squares of ``finalise``'s partial-sum tree, which only its report uses."""
     import ctypes
     import hashlib
     import subprocess
@@ -695,9 +714,25 @@ def _cpu_cupy():
         setattr(cp, name, wrap(getattr(np, name)))
     cp.asnumpy = np.asarray
     cp.ndarray = np.ndarray
+    cp.get_array_module = lambda *a: np
     cp.linalg = types.SimpleNamespace(inv=wrap(np.linalg.inv), norm=np.linalg.norm)
-    cp.cuda = types.SimpleNamespace(Device=lambda *a: types.SimpleNamespace(id=0))
-    cp.RawKernel = RawKernel
+    nothing = lambda *a, **k: None                                   # noqa: E731
+    cp.cuda = types.SimpleNamespace(
+        Device=lambda *a: types.SimpleNamespace(id=0, mem_info=(64 << 30, 64 << 30),
+                                                synchronize=nothing),
+        runtime=types.SimpleNamespace(deviceSynchronize=nothing),
+        get_current_stream=lambda: types.SimpleNamespace(synchronize=nothing, ptr=0))
+    cp.get_default_memory_pool = lambda: types.SimpleNamespace(
+        free_all_blocks=nothing, used_bytes=lambda: 0, free_bytes=lambda: 0)
+
+    class RawModule:
+        def __init__(self, code, options=()):
+            self.code = code
+
+        def get_function(self, name):
+            return RawKernel(self.code, name)
+
+    cp.RawKernel, cp.RawModule = RawKernel, RawModule
     return cp
 
 
@@ -875,7 +910,70 @@ def boundary_case() -> dict:
     return out
 
 
+def gpu_path_case() -> dict:
+    """The reference's device solver (``GPUSolver``, ``zvcfd/fv/solver.py``: fast kernels, fused
+    boundary pass, SuperLU on the host as its ``host-direct`` tests use) run on the CPU through
+    :func:`_cpu_cupy`, on the pipe of its boundary tests (``tests/test_fv_boundaries.py:37-49``)
+    with what only that path has: an RCR outlet coupled implicitly (``:86-109``), an
+    average-static-pressure outlet (``:236-250``) and an opening inlet (``:253-266``). First
+    the harness itself is held to the reference's CPU solver on the golden pipe (same fields to
+    1e-13). Recorded per case: the converged ``U``, ``P`` and the zone flows and pressures."""
+    sys.modules["cupy"] = _cpu_cupy()
+    import os
+
+    os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
+    from zvcfd.fv.solver import GPUSolver
+    from zvcfd.lumped import RCR
+
+    R = 0.5
+    m = tube(R, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed", layers=1)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    fluid = Fluid(1.0, 0.2)
+
+    def run(bcs, tol):
+        s = GPUSolver(m, fluid, bcs, linear="host-direct", linear_rtol=0.0, advection=1.0)
+        rep = s.solve(max_iterations=300, tol=tol)
+        assert rep.converged
+        f = s.fields()
+        return s, f
+
+    # the harness: the golden pipe (parabolic inlet) as the CPU solver converged it
+    g = np.load(HERE / "pipe_reference_tube.npz")
+
+    def prof(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+        return np.stack([0 * r2, 0 * r2, 2 * np.clip(1 - r2, 0, None)], 1)
+
+    _, f = run({z["inlet"]: {"kind": "velocity", "value": prof},
+                z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}},
+               1e-12)
+    assert np.abs(f["U"] - g["U"]).max() < 1e-13 * np.abs(g["U"]).max()
+    out = {}
+    cases = {
+        "rcr": {z["inlet"]: {"kind": "velocity", "flow_rate": 0.3, "profile": "poiseuille"},
+                z["outlet"]: {"kind": "pressure", "lumped": RCR(rp=2.0, c=0.1, rd=5.0, pv=1.0)},
+                z["wall"]: {"kind": "wall"}},
+        "average": {z["inlet"]: {"kind": "velocity", "flow_rate": 0.3},
+                    z["outlet"]: {"kind": "pressure", "value": 2.0, "profile": "average"},
+                    z["wall"]: {"kind": "wall"}},
+        "opening": {z["inlet"]: {"kind": "pressure", "value": 1.0, "opening": True},
+                    z["outlet"]: {"kind": "pressure", "value": 0.0}, z["wall"]: {"kind": "wall"}},
+    }
+    for tag, bcs in cases.items():
+        s, f = run(bcs, 1e-11)
+        q, p = s.patch_flows(), s.patch_pressures()
+        zids = sorted(q)
+        out.update({f"{tag}_U": f["U"], f"{tag}_P": f["P"], f"{tag}_zones": np.array(zids),
+                    f"{tag}_flows": np.array([q[k] for k in zids]),
+                    f"{tag}_pressures": np.array([p[k] for k in zids])})
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["gpu_path"]:
+        np.savez_compressed(HERE / "gpu_path.npz", **gpu_path_case())
+        print("wrote gpu_path")
+        return
     if sys.argv[1:] == ["boundary"]:
         np.savez_compressed(HERE / "boundary_pass.npz", **boundary_case())
         print("wrote boundary_pass")
@@ -979,6 +1077,8 @@ def main():
     print("wrote acm")
     np.savez_compressed(HERE / "boundary_pass.npz", **boundary_case())
     print("wrote boundary_pass")
+    np.savez_compressed(HERE / "gpu_path.npz", **gpu_path_case())
+    print("wrote gpu_path")
 
 
 if __name__ == "__main__":
