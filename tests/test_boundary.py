@@ -104,8 +104,13 @@ def test_prescribed_outlet_gradient_traction_matches_oracle(transpose):
         Boundary(m, bad, 1.0)
 
 
-@pytest.mark.parametrize("extra", [{"profile": "average"}, {"opening": True}])
-def test_unsupported_pressure_zones_are_refused(extra):
+@pytest.mark.parametrize("extra,kind", [({"profile": "average"}, "average"),
+                                        ({"opening": True}, "opening")])
+def test_average_pressure_and_opening_zones(extra, kind):
+    """Zones whose pressures the solve sets each iteration (the reference's device solver,
+    ``zvcfd/fv/solver.py:25-47``): reported as such, their pressure force left out of the fixed
+    outlet force (it comes with the iteration's pressures), and refused where they share nodes
+    with another pressure zone (``:315-318``)."""
     from zvcfd_b200.boundary import Boundary
     from zvcfd_b200.mesh import box
 
@@ -113,9 +118,17 @@ def test_unsupported_pressure_zones_are_refused(extra):
     z = {zz.name: k for k, zz in m.zones.items()}
     bcs = {k: {"kind": "wall"} for k in m.zones}
     bcs[z["xmin"]] = {"kind": "velocity", "value": (1.0, 0.0, 0.0)}
-    bcs[z["xmax"]] = {"kind": "pressure", "value": 0.0, **extra}
-    with pytest.raises(NotImplementedError):
-        Boundary(m, bcs, 1.0)
+    bcs[z["xmax"]] = {"kind": "pressure", "value": 3.0, **extra}
+    bc = Boundary(m, bcs, 1.0)
+    assert bc.special_zones() == {z["xmax"]: kind}
+    assert not bc.outlet_force().any()
+    plain = dict(bcs)
+    plain[z["xmax"]] = {"kind": "pressure", "value": 3.0}
+    assert Boundary(m, plain, 1.0).outlet_force().any()
+    shared = dict(bcs)
+    shared[z["ymin"]] = {"kind": "pressure", "value": 0.0}
+    with pytest.raises(ValueError, match="share nodes"):
+        Boundary(m, shared, 1.0)
 
 
 def test_symmetry_and_pinned_pressure():

@@ -158,6 +158,7 @@ def test_solver_zone_forces_glue_on_cpu_tensors(tag):
     sv.pattern, sv._rawoff, sv.rawdata, sv.rawb = (ip, ix), rawoff, rawdata, rawb.reshape(-1)
     sv.U, sv.P = torch.as_tensor(s.U), torch.as_tensor(s.P)
     sv.bc, sv.stokes, sv._lumped, sv._assembled, sv._raw_rows = bc, False, {}, True, None
+    sv._special = {}
     F = sv.zone_forces()
     got = np.array([F[int(z)] for z in sub["force_zones"]])
     np.testing.assert_allclose(got, sub["forces"], atol=1e-12 * np.abs(sub["forces"]).max())

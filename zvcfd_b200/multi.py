@@ -34,8 +34,8 @@ Morton order; halo rows between ranks travel as point-to-point sends and receive
 per exchange, in the same global order on every rank), and inner products, scales and
 statistics are all-reduced. Every rank builds the same partitions from the same mesh.
 
-Not supported across partitions, as in the reference: average-pressure zones (the build has
-none), eddy viscosity.
+Not supported across partitions: average-pressure zones (as in the reference: their mean
+couples a zone globally), openings, eddy viscosity.
 """
 
 from __future__ import annotations
@@ -277,6 +277,9 @@ class PartBoundary:
     def lumped_zones(self) -> list:
         return self.g.lumped_zones()
 
+    def special_zones(self) -> dict:
+        return self.g.special_zones()
+
     def has_pressure_zone(self) -> bool:
         return self.g.has_pressure_zone()
 
@@ -397,8 +400,11 @@ class B200MultiSolver:
                  maxiter=200, rebuild_every=10, store_geometry="auto", eliminate=True):
         t0 = time.time()
         for zid, spec in bcs.items():
-            if spec.get("profile") == "average":
-                raise NotImplementedError(f"zone {zid}: average-pressure zones need one partition")
+            if spec.get("profile") == "average" or spec.get("opening"):
+                # an average's mean couples the zone globally; an opening's halo nodes would be
+                # eliminated from owned rows with their owner's last value
+                raise NotImplementedError(f"zone {zid}: average-pressure and opening zones "
+                                          "need one partition")
         self.mesh, self.fluid, self.bcs, self.source = mesh, fluid, bcs, source
         self.advection, self.dt, self.stokes = advection, dt, bool(stokes)
         self.rhie_chow, self.freeze_limiter = float(rhie_chow), freeze_limiter
