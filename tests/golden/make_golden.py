@@ -23,7 +23,8 @@ local meshes and halo plans of the reference's partitioner (``partition``); elem
 the reference's device colouring ``gpu_colour`` run on the CPU (``colour``); the reference's ACM
 levels, V-cycle and ACM-FGMRES solve on a system its CPU solver assembled (``acm``); its
 device boundary pass run on the CPU (``boundary``); its whole device solver run on the CPU for
-the RCR outlet, the average-pressure outlet and the opening (``gpu_path``). A single file is
+the RCR outlet, the average-pressure outlet and the opening (``gpu_path``), and for BDF2 steps
+of the RCR outlet (``gpu_path_transient``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -969,7 +970,43 @@ def gpu_path_case() -> dict:
     return out
 
 
+def gpu_path_transient_case() -> dict:
+    """The reference's device solver run on the CPU (as :func:`gpu_path_case`) on its transient
+    RCR test (``tests/test_fv_boundaries.py:112-129``), shortened for the CPU: the pipe with a
+    pulsing flow-rate inlet ``Q(t) = 0.3 + 0.1 sin(2 pi t)`` and an RCR outlet, solved steady to
+    1e-11, then 3 BDF2 steps of 0.05 with up to 20 coefficient loops to 1e-12. Recorded per
+    step: the time, the outlet's flow and pressure; and the final ``U``, ``P``."""
+    sys.modules["cupy"] = _cpu_cupy()
+    import os
+
+    os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
+    from zvcfd.fv.solver import GPUSolver
+    from zvcfd.lumped import RCR
+
+    m = tube(0.5, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed", layers=1)
+    z = {zz.name: k for k, zz in m.zones.items()}
+
+    def Q(t):
+        return 0.3 + 0.1 * np.sin(2 * np.pi * t)
+
+    bcs = {z["inlet"]: {"kind": "velocity", "flow_rate": Q, "profile": "poiseuille"},
+           z["outlet"]: {"kind": "pressure", "lumped": RCR(rp=2.0, c=0.1, rd=5.0, pv=1.0)},
+           z["wall"]: {"kind": "wall"}}
+    s = GPUSolver(m, Fluid(1.0, 0.2), bcs, linear="host-direct", linear_rtol=0.0, advection=1.0)
+    assert s.solve(max_iterations=300, tol=1e-11).converged
+    rec = []
+    s.solve_transient(0.05, 3, loops=20, tol=1e-12,
+                      callback=lambda sv: rec.append((sv.t, sv.patch_flows()[z["outlet"]],
+                                                      sv.patch_pressures()[z["outlet"]])))
+    f = s.fields()
+    return {"steps": np.array(rec), "U": f["U"], "P": f["P"]}
+
+
 def main():
+    if sys.argv[1:] == ["gpu_path_transient"]:
+        np.savez_compressed(HERE / "gpu_path_transient.npz", **gpu_path_transient_case())
+        print("wrote gpu_path_transient")
+        return
     if sys.argv[1:] == ["gpu_path"]:
         np.savez_compressed(HERE / "gpu_path.npz", **gpu_path_case())
         print("wrote gpu_path")
@@ -1079,6 +1116,8 @@ def main():
     print("wrote boundary_pass")
     np.savez_compressed(HERE / "gpu_path.npz", **gpu_path_case())
     print("wrote gpu_path")
+    np.savez_compressed(HERE / "gpu_path_transient.npz", **gpu_path_transient_case())
+    print("wrote gpu_path_transient")
 
 
 if __name__ == "__main__":

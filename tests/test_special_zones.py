@@ -8,7 +8,10 @@ tests (``tests/test_fv_boundaries.py:37-49``) with:
 
 - an RCR outlet coupled implicitly (``:86-109``);
 - an average-static-pressure outlet (``:236-250``);
-- an opening inlet (``:253-266``).
+- an opening inlet (``:253-266``);
+
+and ``tests/golden/gpu_path_transient.npz`` its BDF2 steps of the RCR outlet under a pulsing
+inflow (``:112-129``, shortened to 3 steps).
 
 The oracle must reach the same solutions (the converged outer loops agree to their tolerance:
 1e-9 of the largest velocity and of the pressure range), and the device path's two new pieces,
@@ -98,3 +101,37 @@ def test_device_zone_pressures_equal_the_oracle(tag):
     np.testing.assert_allclose(got.numpy(), want, rtol=0, atol=1e-14 * max(np.abs(want).max(), 1))
     if tag == "opening":
         assert (s._mb[geo["nodes"]] < 0).any()      # some of the zone takes inflow
+
+
+def test_oracle_rcr_march_equals_the_reference_device_march():
+    """The reference's transient RCR test (``tests/test_fv_boundaries.py:112-129``), shortened:
+    BDF2 steps of a pulsing inlet into an RCR outlet. The oracle's step flows, the outlet
+    pressure and the final fields equal the reference device solver's (run on the CPU) to the
+    loops' tolerance."""
+    from zvcfd_b200.lumped import RCR
+
+    T = load("gpu_path_transient")
+    seen = []
+
+    class Recording(RCR):
+        def advance(self, q, t, dt):
+            seen.append((t, q))
+            return super().advance(q, t, dt)
+
+    m, z, bcs, fluid = _case("rcr")
+    bcs[z["inlet"]] = {"kind": "velocity", "flow_rate": lambda t: 0.3 + 0.1 * np.sin(2 * np.pi * t),
+                       "profile": "poiseuille"}
+    bcs[z["outlet"]] = {"kind": "pressure", "lumped": Recording(rp=2.0, c=0.1, rd=5.0, pv=1.0)}
+    s = OracleSolver(m, fluid, bcs, advection=1.0)
+    assert s.solve(max_iterations=300, tol=1e-11)["converged"]
+    s.solve_transient(0.05, 3, loops=20, tol=1e-12)
+    steps = T["steps"]                                  # (t, outlet flow, outlet pressure)
+    assert len(seen) == len(steps) == 3
+    for (t, q), (tr, qr, pr) in zip(seen, steps):
+        assert abs(t - tr) < 1e-15 and abs(q - qr) < 1e-9 * 0.3
+    f, S = s.sub[z["outlet"]]
+    ok = f >= 0
+    a = np.linalg.norm(S, axis=2) * ok
+    assert abs(float((s.P[np.where(ok, f, 0)] * a).sum() / a.sum()) - steps[-1][2]) < 1e-9
+    np.testing.assert_allclose(s.U, T["U"], rtol=0, atol=1e-9 * np.abs(T["U"]).max())
+    np.testing.assert_allclose(s.P, T["P"], rtol=0, atol=1e-9 * np.ptp(T["P"]))
