@@ -918,7 +918,8 @@ def gpu_path_case() -> dict:
     with what only that path has: an RCR outlet coupled implicitly (``:86-109``), an
     average-static-pressure outlet (``:236-250``) and an opening inlet (``:253-266``). First
     the harness itself is held to the reference's CPU solver on the golden pipe (same fields to
-    1e-13). Recorded per case: the converged ``U``, ``P`` and the zone flows and pressures."""
+    1e-13). Recorded per case: the converged ``U``, ``P``, the zone flows, pressures and forces,
+    and the wall shear stress from consistent reactions."""
     sys.modules["cupy"] = _cpu_cupy()
     import os
 
@@ -964,9 +965,13 @@ def gpu_path_case() -> dict:
         s, f = run(bcs, 1e-11)
         q, p = s.patch_flows(), s.patch_pressures()
         zids = sorted(q)
+        forces = s.zone_forces()
+        nodes, tau = s.wall_shear("reaction")
         out.update({f"{tag}_U": f["U"], f"{tag}_P": f["P"], f"{tag}_zones": np.array(zids),
                     f"{tag}_flows": np.array([q[k] for k in zids]),
-                    f"{tag}_pressures": np.array([p[k] for k in zids])})
+                    f"{tag}_pressures": np.array([p[k] for k in zids]),
+                    f"{tag}_forces": np.array([forces[k] for k in zids]),
+                    f"{tag}_shear_nodes": np.asarray(nodes), f"{tag}_shear": np.asarray(tau)})
     return out
 
 

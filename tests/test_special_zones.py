@@ -135,3 +135,30 @@ def test_oracle_rcr_march_equals_the_reference_device_march():
     assert abs(float((s.P[np.where(ok, f, 0)] * a).sum() / a.sum()) - steps[-1][2]) < 1e-9
     np.testing.assert_allclose(s.U, T["U"], rtol=0, atol=1e-9 * np.abs(T["U"]).max())
     np.testing.assert_allclose(s.P, T["P"], rtol=0, atol=1e-9 * np.ptp(T["P"]))
+
+
+@pytest.mark.parametrize("tag", ["rcr", "average", "opening"])
+def test_device_path_forces_on_these_zones(tag):
+    """Zone forces and wall shear from consistent reactions, by the device path's host code
+    (``zvcfd_b200.forces`` over the kept rows in the boundary pass's layout) on the oracle's
+    converged state, against the reference device solver's own: a lumped, average-pressure or
+    opening zone's pressure force takes the nodal pressures."""
+    from test_forces import _compact
+    from zvcfd_b200.boundary import Boundary
+    from zvcfd_b200.forces import RawRows, wall_shear_reaction, zone_forces
+
+    m, z, bcs, fluid = _case(tag)
+    s = OracleSolver(m, fluid, bcs, advection=1.0)
+    assert s.solve(max_iterations=300, tol=1e-11)["converged"]
+    bc = Boundary(m, bcs, fluid.rho, mu=fluid.mu)
+    raw = RawRows(*_compact(s, bc.vel_fixed_comp.any(1)))
+    r = raw.residual(torch.as_tensor(np.concatenate([s.U, s.P[:, None]], 1))).numpy()
+    nodal = list(bc.lumped_zones()) + list(bc.special_zones())
+    F = zone_forces(bc, r, s.P, lumped=nodal)
+    want = G[f"{tag}_forces"]
+    got = np.array([F[int(k)] for k in G[f"{tag}_zones"]])
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-9 * np.abs(want).max())
+    nodes, tau = wall_shear_reaction(bc, r, s.P)
+    np.testing.assert_array_equal(nodes, G[f"{tag}_shear_nodes"])
+    ref = G[f"{tag}_shear"]
+    np.testing.assert_allclose(tau, ref, rtol=0, atol=1e-9 * np.abs(ref).max())
