@@ -24,7 +24,8 @@ the reference's device colouring ``gpu_colour`` run on the CPU (``colour``); the
 levels, V-cycle and ACM-FGMRES solve on a system its CPU solver assembled (``acm``); its
 device boundary pass run on the CPU (``boundary``); its whole device solver run on the CPU for
 the RCR outlet, the average-pressure outlet and the opening (``gpu_path``), and for BDF2 steps
-of the RCR outlet (``gpu_path_transient``). A single file is
+of the RCR outlet (``gpu_path_transient``); the CPU solver's second-order boundary
+reconstruction (``reconstruction``). A single file is
 rewritten by naming it (``python tests/golden/make_golden.py forces``). Nothing
 at test or bench time reads the reference: the tests read these files.
 """
@@ -1007,7 +1008,47 @@ def gpu_path_transient_case() -> dict:
     return {"steps": np.array(rec), "U": f["U"], "P": f["P"]}
 
 
+def reconstruction_case() -> dict:
+    """The reference CPU solver's opt-in second-order boundary reconstruction
+    (``boundary_reconstruction = True``, ``zvcfd/fv/reference.py:766-790``,
+    ``zvcfd/fv/boundary_advection.py:167-219``) on the golden pipe (its own boundary tests'
+    tube): the raw system after three outer iterations with a fixed blend, and the converged
+    fields with a fixed blend and with High Resolution."""
+    R = 0.5
+    m = tube(R, 2.0, n_core=2, n_ring=2, n_axial=8, kind="mixed", layers=1)
+    zid = {z.name: k for k, z in m.zones.items()}
+
+    def prof(x):
+        r2 = (x[:, 0] ** 2 + x[:, 1] ** 2) / R ** 2
+        return np.stack([0 * r2, 0 * r2, 2 * np.clip(1 - r2, 0, None)], 1)
+
+    def bcs():
+        return {zid["inlet"]: {"kind": "velocity", "value": prof},
+                zid["outlet"]: {"kind": "pressure", "value": 0.0}, zid["wall"]: {"kind": "wall"}}
+
+    out = {}
+    s = ReferenceSolver(m, Fluid(1.0, 0.2), bcs(), advection=1.0, lag_rhie_chow=True)
+    s.boundary_reconstruction = True
+    s.solve(max_iterations=3, tol=0.0)
+    s.assemble()
+    M, b = s._raw
+    indptr, indices = node_graph(m)
+    out.update(raw=blocks_on_pattern(M, indptr, indices), braw=b.reshape(-1, 4),
+               U3=s.U.copy(), P3=s.P.copy(), mb3=s._mb.copy())
+    for tag, adv in (("blend", 1.0), ("hr", "high-resolution")):
+        s = ReferenceSolver(m, Fluid(1.0, 0.2), bcs(), advection=adv, lag_rhie_chow=True)
+        s.boundary_reconstruction = True
+        rep = s.solve(max_iterations=400, tol=1e-12)
+        assert rep.converged
+        out.update({f"{tag}_U": s.U, f"{tag}_P": s.P, f"{tag}_iterations": np.array(rep.iterations)})
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["reconstruction"]:
+        np.savez_compressed(HERE / "reconstruction.npz", **reconstruction_case())
+        print("wrote reconstruction")
+        return
     if sys.argv[1:] == ["gpu_path_transient"]:
         np.savez_compressed(HERE / "gpu_path_transient.npz", **gpu_path_transient_case())
         print("wrote gpu_path_transient")
@@ -1123,6 +1164,8 @@ def main():
     print("wrote gpu_path")
     np.savez_compressed(HERE / "gpu_path_transient.npz", **gpu_path_transient_case())
     print("wrote gpu_path_transient")
+    np.savez_compressed(HERE / "reconstruction.npz", **reconstruction_case())
+    print("wrote reconstruction")
 
 
 if __name__ == "__main__":
