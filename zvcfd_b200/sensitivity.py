@@ -120,6 +120,9 @@ class SteadyResidual:
         if s.dt or s._time is not None:
             raise ValueError("the adjoint is of the steady state or of BDF steps, not of a "
                              "false time step")
+        if getattr(s, "_special", None) or getattr(s, "boundary_reconstruction", False):
+            raise NotImplementedError("the restated residual has no average-pressure or opening "
+                                      "zones and no boundary reconstruction")
         self.s = s
         self.rho = float(s.fluid.rho)
         self.visc = s.fluid.viscosity
