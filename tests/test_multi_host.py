@@ -231,3 +231,18 @@ def test_fgmres_edge_cases():
     assert ok and it > 5 and res <= 1.01e-10
     want = np.linalg.solve(M.numpy(), b.numpy())
     assert np.abs(x.numpy() - want).max() <= 1e-8 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("extra", [{"profile": "average"}, {"opening": True}])
+def test_partitioned_solver_refuses_zones_that_couple_partitions(extra):
+    """An average-pressure zone's mean couples it globally, and an opening's halo nodes would
+    be eliminated with stale values: the partitioned solver refuses both before it sets up."""
+    from zvcfd_b200.fluid import Fluid
+    from zvcfd_b200.multi import B200MultiSolver
+
+    g, m, owner, local, plan = _case(2)
+    bcs = pipe_bcs("pipe_reference_tube", g, m)
+    z = {zz.name: k for k, zz in m.zones.items()}
+    bcs[z["outlet"]] = {"kind": "pressure", "value": 0.0, **extra}
+    with pytest.raises(NotImplementedError, match="one partition"):
+        B200MultiSolver(m, Fluid(1.0, 0.2), bcs, parts=2)
